@@ -1,0 +1,300 @@
+// Test infrastructure (oracle): a C-ABI driver around the unmodified DollarStoreSCF
+// sources, compiled by oracle/build_ref.sh into oracle/_ref/libdssref.so.
+// The reference ships no main() and no tests; this file is the driver its README
+// expects a user to write.  It is never linked into the product library.
+//
+// Every entry point drives the reference's own functions:
+//   molecule / basis      scf::assignMolecule      chem/scf/SCFBasis.cpp:17-37
+//   spherical basis       scf::constructBasis      chem/scf/SCFBasis.cpp:107-171
+//   Cartesian (6D) basis  the same steps with one Cartesian term per function
+//                         (the reference has no 6D mode; chem/GTO.cpp:15-94 builds
+//                         only real solid harmonics)
+//   SCF                   scf::useCoreGuess + scf::solveMOs + scf::getTotalEnergy
+//                         chem/scf/SCFSolver.cpp:179-237, chem/scf/Energy.cpp:21-78
+//   Fock two-electron     scf::computeCoulombTerms / computeExchangeTerms
+//                         chem/scf/SCFSolver.cpp:29-43 over the stored tensor of
+//                         chem/scf/ExactCoulomb.cpp:41-72
+//   single ERI            flo::electronRepulsionIntegral chem/GaussianIntegral.cpp:561-642
+//   Boys                  flo::boysFunctionExact     chem/GaussianIntegral.cpp:209-223
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <iostream>
+#include <sstream>
+#include <vector>
+
+#include "chem/GTO.hpp"
+#include "chem/GaussianIntegral.hpp"
+#include "chem/Molecule.hpp"
+#include "chem/scf/Energy.hpp"
+#include "chem/scf/ExactCoulomb.hpp"
+#include "chem/scf/SCFBasis.hpp"
+#include "chem/scf/SCFCommon.hpp"
+#include "chem/scf/SCFSolver.hpp"
+
+namespace flo {
+double boysFunctionExact(double x, uint m);
+}
+namespace scf {
+extern flo::Molecule molecule;
+extern std::vector<flo::AtomicBasis> atom_bases;
+extern double energy_threshold;
+extern uint iteration;
+void assignOverlapMatrix();
+void assignCoreHamiltonian();
+void assignOrthogonalization();
+}  // namespace scf
+
+namespace {
+std::stringstream g_sink;
+std::streambuf* g_saved = nullptr;
+void quiet_on() {
+  if (!g_saved) g_saved = std::cout.rdbuf(g_sink.rdbuf());
+  g_sink.str("");
+}
+void quiet_off() {
+  if (g_saved) std::cout.rdbuf(g_saved);
+  g_saved = nullptr;
+}
+
+double dfact(int n) {
+  double r = 1.0;
+  for (int i = n; i > 0; i -= 2) r *= i;
+  return r;
+}
+
+bool g_have_tensor = false;
+
+// Fill scf::basis the way constructBasis() does (SCFBasis.cpp:120-139), but with
+// one Cartesian monomial per function in 6D mode.  Monomials of a shell are
+// ordered x-major: for l=2 xx, xy, xz, yy, yz, zz.
+void build_basis_6d() {
+  using namespace scf;
+  basis.clear();
+  basis_atoms.clear();
+  atom_basis.clear();
+  atom_basis.push_back(0);
+  for (size_t i = 0; i < molecule.size(); ++i) {
+    flo::vec3 center = molecule[i].position;
+    for (flo::GTOShell& shell : atom_bases[i]) {
+      int l = (int)shell.l;
+      for (int a = l; a >= 0; --a) {
+        for (int b = l - a; b >= 0; --b) {
+          int c = l - a - b;
+          flo::ContractedGaussian g(shell.primitives, (uint)l, 0, center);
+          double w = std::sqrt(dfact(2 * l + 1) /
+                               (4.0 * PI * dfact(2 * a - 1) * dfact(2 * b - 1) * dfact(2 * c - 1)));
+          g.spherical_harmonic.clear();
+          g.spherical_harmonic.push_back(flo::CartesianPolynomialTerm(w, (uint)a, (uint)b, (uint)c));
+          basis.push_back(g);
+          basis_atoms.push_back((uint)i);
+        }
+      }
+    }
+    atom_basis.push_back((uint)basis.size());
+  }
+}
+
+// Buffer sizing of constructBasis() (SCFBasis.cpp:142-162), then S, H, X.
+void size_state_and_one_electron() {
+  using namespace scf;
+  matrix_size = (uint)basis.size();
+  buffer.resize(5);
+  asymmetric_buffer.resize(5);
+  for (int i = 0; i < 5; ++i) {
+    buffer[i].resize(basis.size());
+    asymmetric_buffer[i].resize(basis.size(), basis.size());
+  }
+  fock_matrix[0].resize(matrix_size);
+  two_electron_hamiltonian[0].resize(matrix_size);
+  coefficient_matrix[0].resize(matrix_size, matrix_size);
+  density_matrix[0].resize(basis.size());
+  total_density_matrix.resize(basis.size());
+  assignOverlapMatrix();
+  assignCoreHamiltonian();
+  assignOrthogonalization();
+}
+
+void copy_packed(const flo::SymmetricMatrixNd& m, double* out) {
+  size_t n = m.getWidth();
+  for (size_t x = 0; x < n; ++x)
+    for (size_t y = 0; y <= x; ++y) out[x * (x + 1) / 2 + y] = m.at((uint)y, (uint)x);
+}
+void load_packed(flo::SymmetricMatrixNd& m, const double* in) {
+  size_t n = m.getWidth();
+  for (size_t x = 0; x < n; ++x)
+    for (size_t y = 0; y <= x; ++y) m.at((uint)y, (uint)x) = in[x * (x + 1) / 2 + y];
+}
+}  // namespace
+
+extern "C" {
+
+// Molecule and basis.  Z[natom], xyz_bohr[3*natom]; shells in atom order with
+// shell_atom[s], shell_l[s], shell_nprim[s], then exps/coefs concatenated.
+// cartesian: 0 = the reference's spherical (5D) functions, 1 = 6D monomials.
+// build_tensor: 1 = also build the stored ERI tensor (needed for SCF/Fock).
+// Returns the number of basis functions.
+int ref_setup(int natom, const int* Z, const double* xyz_bohr, int nshell, const int* shell_atom,
+              const int* shell_l, const int* shell_nprim, const double* exps, const double* coefs,
+              int charge, int multiplicity, int cartesian, int build_tensor, int quiet) {
+  if (quiet) quiet_on();
+  flo::Molecule mol;
+  for (int i = 0; i < natom; ++i) {
+    flo::vec3 p(xyz_bohr[3 * i], xyz_bohr[3 * i + 1], xyz_bohr[3 * i + 2]);
+    mol.atoms.push_back(flo::Atom(p, (flo::Element)Z[i]));
+  }
+  scf::assignMolecule(mol, charge, (uint)multiplicity);
+  int off = 0;
+  for (int s = 0; s < nshell; ++s) {
+    std::vector<flo::GTOPrimitive> prims;
+    for (int k = 0; k < shell_nprim[s]; ++k) prims.push_back(flo::GTOPrimitive(exps[off + k], coefs[off + k]));
+    off += shell_nprim[s];
+    scf::atom_bases[shell_atom[s]].push_back(flo::GTOShell((uint)shell_l[s], prims));
+  }
+  g_have_tensor = false;
+  if (!cartesian && build_tensor) {
+    scf::constructBasis();
+    g_have_tensor = true;
+  } else {
+    if (cartesian) {
+      build_basis_6d();
+    } else {
+      // constructBasis() without the tensor: the same function list.
+      scf::basis.clear();
+      scf::basis_atoms.clear();
+      scf::atom_basis.clear();
+      scf::atom_basis.push_back(0);
+      for (size_t i = 0; i < scf::molecule.size(); ++i) {
+        for (flo::GTOShell& sh : scf::atom_bases[i])
+          for (int m = -(int)sh.l; m <= (int)sh.l; ++m) {
+            scf::basis.push_back(flo::ContractedGaussian(sh.primitives, sh.l, m, scf::molecule[i].position));
+            scf::basis_atoms.push_back((uint)i);
+          }
+        scf::atom_basis.push_back((uint)scf::basis.size());
+      }
+    }
+    size_state_and_one_electron();
+    if (build_tensor) {
+      scf::assignExactRepulsionTensor();
+      g_have_tensor = true;
+    }
+  }
+  if (quiet) quiet_off();
+  return (int)scf::basis.size();
+}
+
+int ref_nbf() { return (int)scf::basis.size(); }
+
+// Packed-upper (LAPACK 'U') one-electron matrices.
+void ref_get_overlap(double* out) { copy_packed(scf::overlap_matrix, out); }
+void ref_get_core_hamiltonian(double* out) { copy_packed(scf::core_hamiltonian, out); }
+
+// Cartesian terms of basis function f: returns the count, fills (weight, x, y, z).
+int ref_basis_terms(int f, double* weight, int* xyz) {
+  const flo::ContractedGaussian& g = scf::basis[f];
+  for (size_t t = 0; t < g.spherical_harmonic.size(); ++t) {
+    weight[t] = g.spherical_harmonic[t].weight;
+    xyz[3 * t] = (int)g.spherical_harmonic[t].x;
+    xyz[3 * t + 1] = (int)g.spherical_harmonic[t].y;
+    xyz[3 * t + 2] = (int)g.spherical_harmonic[t].z;
+  }
+  return (int)g.spherical_harmonic.size();
+}
+// Normalised primitive weights of basis function f (chem/GTO.cpp:90-93).
+int ref_basis_prims(int f, double* zeta, double* weight) {
+  const flo::ContractedGaussian& g = scf::basis[f];
+  for (size_t p = 0; p < g.primitives.size(); ++p) {
+    zeta[p] = g.primitives[p].zeta;
+    weight[p] = g.primitives[p].weight;
+  }
+  return (int)g.primitives.size();
+}
+
+// RHF SCF from the core guess to |dE| < conv.  Returns the iteration count;
+// fills E_total and the final alpha density (packed-U).
+int ref_scf(double conv, double* E_total, double* D_alpha_packed, double* seconds, int quiet) {
+  if (!g_have_tensor) return -1;
+  if (quiet) quiet_on();
+  scf::energy_threshold = conv;
+  auto t0 = std::chrono::steady_clock::now();
+  scf::useCoreGuess();
+  scf::solveMOs();
+  auto t1 = std::chrono::steady_clock::now();
+  *E_total = scf::getTotalEnergy();
+  if (D_alpha_packed) copy_packed(scf::density_matrix[0], D_alpha_packed);
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (quiet) quiet_off();
+  return (int)scf::iteration;
+}
+
+// Two-electron Fock part for a given alpha density: G = J[2 D_alpha] - K[D_alpha]
+// (the RHF G of SCFSolver.cpp:29-43, computeDensityMatrix :92).
+int ref_fock_2e(const double* D_alpha_packed, double* G_packed) {
+  if (!g_have_tensor) return -1;
+  load_packed(scf::density_matrix[0], D_alpha_packed);
+  scf::total_density_matrix = 2.0 * scf::density_matrix[0];
+  scf::computeCoulombTerms(scf::Spin::alpha);
+  scf::computeExchangeTerms(scf::Spin::alpha);
+  copy_packed(scf::two_electron_hamiltonian[0], G_packed);
+  return 0;
+}
+
+// J[D_total] and K[D_alpha] separately (packed-U), from the stored tensor.
+int ref_jk(const double* D_alpha_packed, double* J_packed, double* K_packed) {
+  if (!g_have_tensor) return -1;
+  size_t n = scf::basis.size();
+  load_packed(scf::density_matrix[0], D_alpha_packed);
+  scf::total_density_matrix = 2.0 * scf::density_matrix[0];
+  for (uint mu = 0; mu < n; ++mu)
+    for (uint nu = mu; nu < n; ++nu) {
+      J_packed[(size_t)nu * (nu + 1) / 2 + mu] = scf::getExactCoulombMatrix(mu, nu);
+      K_packed[(size_t)nu * (nu + 1) / 2 + mu] = scf::getExactExchangeMatrix(mu, nu, scf::Spin::alpha);
+    }
+  return 0;
+}
+
+// (mu nu | sigma tau) in chemist notation; argument order of the reference is
+// (mu, sigma, nu, tau) (GaussianIntegral.cpp:561-565).
+double ref_eri(int mu, int nu, int sigma, int tau) {
+  return flo::electronRepulsionIntegral(scf::basis[mu], scf::basis[sigma], scf::basis[nu], scf::basis[tau]);
+}
+
+double ref_boys(double x, unsigned m) { return flo::boysFunctionExact(x, m); }
+
+// Timed sample of the ERI phase: the canonical function quartets
+// (i>=j, k>=l, ij<=kl) of assignExactRepulsionTensor (ExactCoulomb.cpp:54-68)
+// whose first index i lies in [i_begin, i_end).  Returns the quartet count and
+// the seconds spent; a checksum of the integrals guards against dead-code removal.
+long long ref_time_eri_rows(int i_begin, int i_end, double* seconds, double* checksum) {
+  size_t n = scf::basis.size();
+  long long count = 0;
+  double sum = 0.0;
+  auto t0 = std::chrono::steady_clock::now();
+  for (uint i = (uint)i_begin; i < (uint)i_end && i < n; ++i)
+    for (uint j = 0; j <= i; ++j)
+      for (uint k = 0; k < n; ++k)
+        for (uint l = 0; l <= k; ++l) {
+          uint m = j + i * (i + 1) / 2;
+          uint nn = l + k * (k + 1) / 2;
+          if (m > nn) continue;
+          sum += flo::electronRepulsionIntegral(scf::basis[i], scf::basis[k], scf::basis[j], scf::basis[l]);
+          ++count;
+        }
+  auto t1 = std::chrono::steady_clock::now();
+  *seconds = std::chrono::duration<double>(t1 - t0).count();
+  *checksum = sum;
+  return count;
+}
+
+// Timed J+K digest over the stored tensor for one density (the per-iteration
+// Fock work of the reference, SCFSolver.cpp:29-43).  Returns seconds.
+double ref_time_jk(const double* D_alpha_packed) {
+  size_t n = scf::basis.size();
+  std::vector<double> G(n * (n + 1) / 2);
+  auto t0 = std::chrono::steady_clock::now();
+  ref_fock_2e(D_alpha_packed, G.data());
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+}  // extern "C"
