@@ -1,0 +1,84 @@
+"""ctypes binding of libdss.so (include/dss.h).
+
+The library is the product; this module only loads it and declares the C
+signatures.  Loading fails loudly when the built library is missing: there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libdss.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "dss.h")
+
+_lib = None
+
+
+class DssError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dss error {code}: {msg}")
+        self.code = code
+
+
+class DssOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("schwarz_threshold", ctypes.c_double), ("boys_mode", ctypes.c_int)]
+
+
+def header_symbols():
+    """Function names declared in include/dss.h."""
+    with open(HEADER) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(dss_\w+)\s*\(", text, flags=re.M)))
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.isfile(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is not built; run `python -m dollarstorescf_b200.build` (there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    L.dss_default_opts.argtypes = [ctypes.POINTER(DssOpts)]
+    L.dss_default_opts.restype = None
+    L.dss_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(DssOpts)]
+    L.dss_create.restype = ctypes.c_int
+    L.dss_destroy.argtypes = [vp]
+    L.dss_destroy.restype = None
+    L.dss_last_error.argtypes = [vp]
+    L.dss_last_error.restype = ctypes.c_char_p
+    L.dss_set_basis.argtypes = [vp, ctypes.c_int, ip, ip, dp, dp, dp, ctypes.c_int]
+    L.dss_set_basis.restype = ctypes.c_int
+    L.dss_nbf.argtypes = [vp]
+    L.dss_nbf.restype = ctypes.c_int
+    L.dss_build_jk.argtypes = [vp, dp, dp, dp]
+    L.dss_build_jk.restype = ctypes.c_int
+    L.dss_build_jk_device.argtypes = [vp, vp, vp, vp]
+    L.dss_build_jk_device.restype = ctypes.c_int
+    L.dss_sync.argtypes = [vp]
+    L.dss_sync.restype = ctypes.c_int
+    L.dss_work_stats.argtypes = [vp, llp, llp, llp]
+    L.dss_work_stats.restype = ctypes.c_int
+    L.dss_set_stream.argtypes = [vp, vp]
+    L.dss_set_stream.restype = ctypes.c_int
+    L.dss_get_stream.argtypes = [vp]
+    L.dss_get_stream.restype = vp
+    L.dss_num_classes.argtypes = []
+    L.dss_num_classes.restype = ctypes.c_int
+    L.dss_class_info.argtypes = [vp, ctypes.c_int, ip, llp, llp, llp]
+    L.dss_class_info.restype = ctypes.c_int
+    L.dss_kernels_per_build.argtypes = [vp]
+    L.dss_kernels_per_build.restype = ctypes.c_int
+    L.dss_profile_build.argtypes = [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_float)]
+    L.dss_profile_build.restype = ctypes.c_int
+    L.dss_probe_fp64_peak.argtypes = [vp, dp]
+    L.dss_probe_fp64_peak.restype = ctypes.c_int
+    _lib = L
+    return L

@@ -1,0 +1,173 @@
+// Boys function F_m(x) = int_0^1 t^(2m) exp(-x t^2) dt, m = 0..L, in two modes.
+//
+// DSS_BOYS_REF reproduces the reference's flo::boysFunctionExact
+// (chem/GaussianIntegral.cpp:209-223) value for value: for x > 1.1 m + 25 the
+// asymptotic form (2m-1)!!/2^(m+1) sqrt(PI/x^(2m+1)) with PI = 3.14159265358979,
+// otherwise exp(-x)/(2m+1) * sum_i a_i with a_0 = 1, a_i = a_(i-1) 2x/(2m+2i+1),
+// summed up to and including the first term <= 1e-9.  That truncation leaves
+// an absolute error of up to ~1.5e-11 which moves (H2O)_16 energies by ~1e-9 Eh,
+// so this mode is the one that meets 1e-9 Eh parity with the reference.  The
+// per-m series share one sequence: the m-series is the (m+1)-series scaled by
+// 2x/(2m+3) plus a leading 1, so the top m runs the full series and each lower m
+// only adjusts its truncation point by a few terms (the stopping rule is applied
+// to the m-series' own terms, exactly as the reference applies it).
+//
+// DSS_BOYS_FAST is the accurate function: a 7-term Taylor expansion of F_L
+// about the nearest point of a 1/16-spaced table (boys_tab.cuh), downward
+// recursion F_m = (2x F_(m+1) + exp(-x)) / (2m+1), and for x >= 36 the
+// asymptotic F_0 = sqrt(pi/x)/2 with upward recursion.  Relative error ~1e-14.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "boys_tab.cuh"
+
+#define DSS_BOYS_REF 0
+#define DSS_BOYS_FAST 1
+
+#define DSS_PI_REF 3.14159265358979
+
+// 1/(2k+1) for k = 0..255 (g_odd_inv in boys_tab.cuh): the series divides
+// 2x/(2m+2i+1) become products with a correctly rounded reciprocal.
+__device__ __forceinline__ double odd_inv(int k) { return g_odd_inv[k]; }
+
+// The reference's integer power (lalib/MathUtil.hpp:56-66): square-and-multiply
+// in its own order, so the asymptotic branch rounds the same way.
+__device__ __forceinline__ double ref_ipow(double x, unsigned p) {
+  // Iterative form of: if p==1 return x; if p==0 return 1; y=x; l=2;
+  // while l<p: y=y*y, l*=2; return y * pow(x, p - l/2) -- the factors are
+  // multiplied innermost first, as the recursion does.
+  double fac[8];
+  int nf = 0;
+  double tail;
+  while (true) {
+    if (p == 0) { tail = 1.0; break; }
+    if (p == 1) { tail = x; break; }
+    double y = x;
+    unsigned l = 2;
+    for (; l < p; l *= 2) y = y * y;
+    fac[nf++] = y;
+    p = p - l / 2;
+  }
+  double r = tail;
+  for (int i = nf - 1; i >= 0; --i) r = fac[i] * r;
+  return r;
+}
+
+template <int L>
+__device__ __forceinline__ void boys_ref(double x, double* F) {
+  const double ex = exp(-x);
+  // m values with x > 1.1 m + 25 take the asymptotic branch; they are the lowest m.
+  // Series for the remaining m are built from the top down.
+  int m_series_lo = L + 1;
+#pragma unroll
+  for (int m = L; m >= 0; --m) {
+    const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
+    if (!(x > thr)) m_series_lo = m;
+  }
+  // Top series (m = L) when it is needed.
+  double S = 0.0, last = 0.0;
+  int n = 0;  // index of the last term included
+  if (m_series_lo <= L) {
+    const double x2 = 2.0 * x;
+    double a = 1.0;
+    S = 1.0;
+    int i = 1;
+    do {
+      a = x2 * odd_inv(L + i) * a;
+      S += a;
+      ++i;
+    } while (a > 0.000000001);
+    n = i - 1;
+    last = a;
+    F[L] = ex * odd_inv(L) * S;
+  }
+  // Downward: the m-series terms are t^(m)_i = c_m t^(m+1)_(i-1) with
+  // c_m = 2x/(2m+3); the reference stops at the first i >= 1 with t^(m)_i <= 1e-9.
+#pragma unroll
+  for (int m = L - 1; m >= 0; --m) {
+    if (m < m_series_lo) break;
+    const double c = 2.0 * x * odd_inv(m + 1);
+    // (m+1)-series: S = sum_{k=0..n} t_k, last = t_n.  Find the first k >= 0 with
+    // c * t_k <= 1e-9 (the m-series stop index is k + 1).
+    double Sm1 = S, t = last;
+    int k = n;
+    if (c * t <= 0.000000001) {
+      // Walk back while the previous term also satisfies the stop rule.
+      while (k > 0) {
+        const double tp = t * (double)(2 * (m + 1) + 2 * k + 1) / (2.0 * x);
+        if (c * tp <= 0.000000001) {
+          Sm1 -= t;
+          t = tp;
+          --k;
+        } else {
+          break;
+        }
+      }
+    } else {
+      // Extend the (m+1)-series forward until the stop rule holds.
+      do {
+        t = t * 2.0 * x * odd_inv(m + 1 + k + 1);
+        Sm1 += t;
+        ++k;
+      } while (c * t > 0.000000001);
+    }
+    // m-series: 1 + c * (sum of (m+1)-terms 0..k), last term c * t_k, stop index k + 1.
+    S = 1.0 + c * Sm1;
+    last = c * t;
+    n = k + 1;
+    F[m] = ex * odd_inv(m) * S;
+  }
+  // Asymptotic branch for the low m.
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if (m < m_series_lo) {
+      // (2m-1)!! in 32-bit int arithmetic as the reference evaluates it
+      // (doubleFactorial<int>, lalib/MathUtil.hpp:36-42); it wraps for m >= 11.
+      unsigned int dfi = 1u;
+      for (int j = 2 * m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
+      const double df = (double)(int)dfi;
+      double p2 = 1.0;
+      for (int j = 0; j < m + 1; ++j) p2 *= 2.0;
+      F[m] = df / p2 * sqrt(DSS_PI_REF / ref_ipow(x, 2 * m + 1));
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void boys_fast(double x, double* F) {
+  if (x < 35.9) {
+    const int k = __double2int_rn(x * (double)DSS_BOYS_STEP);
+    const double dx = (double)k * (1.0 / DSS_BOYS_STEP) - x;  // x0 - x
+    const double* row = g_boys_tab + k * DSS_BOYS_NM + L;
+    // Taylor: F_L(x) = sum_j F_(L+j)(x0) (x0 - x)^j / j!
+    double f = row[6] * (1.0 / 720.0);
+    f = f * dx + row[5] * (1.0 / 120.0);
+    f = f * dx + row[4] * (1.0 / 24.0);
+    f = f * dx + row[3] * (1.0 / 6.0);
+    f = f * dx + row[2] * 0.5;
+    f = f * dx + row[1];
+    f = f * dx + row[0];
+    F[L] = f;
+    if (L > 0) {
+      const double ex = exp(-x);
+      const double x2 = 2.0 * x;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = (x2 * F[m + 1] + ex) * (1.0 / (double)(2 * m + 1));
+    }
+  } else {
+    const double ex = exp(-x);
+    const double inv2x = 0.5 / x;
+    F[0] = 0.5 * sqrt(3.141592653589793 / x);
+#pragma unroll
+    for (int m = 0; m < L; ++m) F[m + 1] = ((double)(2 * m + 1) * F[m] - ex) * inv2x;
+  }
+}
+
+template <int BOYS, int L>
+__device__ __forceinline__ void boys_eval(double x, double* F) {
+  if constexpr (BOYS == DSS_BOYS_REF) {
+    boys_ref<L>(x, F);
+  } else {
+    boys_fast<L>(x, F);
+  }
+}

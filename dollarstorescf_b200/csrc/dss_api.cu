@@ -1,0 +1,593 @@
+// Host side of the C ABI (include/dss.h): basis packing, shell pairs, Schwarz
+// factors, screened work lists and the J/K build driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "dss.h"
+#include "dss_internal.h"
+#include "eri_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr double kPiRef = 3.14159265358979;  // lalib/MathUtil.hpp:8
+
+double dfact(int n) {
+  double r = 1.0;
+  for (int i = n; i > 0; i -= 2) r *= i;
+  return r;
+}
+
+int pair_class_index(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+__global__ void unpack_kernel(const double* __restrict__ packed, double* __restrict__ dense, int n) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * n) return;
+  const int r = (int)(idx / n), c = (int)(idx % n);
+  const int x = r > c ? r : c, y = r > c ? c : r;
+  dense[idx] = packed[(long long)x * (x + 1) / 2 + y];
+}
+
+// out = acc + acc^T (dense) and optionally packed-U.
+__global__ void symmetrize_kernel(const double* __restrict__ acc, double* __restrict__ dense,
+                                  double* __restrict__ packed, int n) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * n) return;
+  const int r = (int)(idx / n), c = (int)(idx % n);
+  const double v = acc[(long long)r * n + c] + acc[(long long)c * n + r];
+  if (dense) dense[idx] = v;
+  if (packed && r <= c) packed[(long long)c * (c + 1) / 2 + r] = v;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ helpers
+int dss_fail(dss_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return DSS_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return dss_fail(ctx, e == cudaErrorMemoryAllocation ? DSS_ERR_OOM : DSS_ERR_CUDA, m);
+}
+
+#define DSS_CUDA(call)                                        \
+  do {                                                        \
+    int _rc = dss_cuda_check(ctx, (call), #call);             \
+    if (_rc != DSS_OK) return _rc;                            \
+  } while (0)
+
+template <class T>
+static int upload(dss_ctx* ctx, DevBuf<T>& buf, const std::vector<T>& host) {
+  DSS_CUDA(buf.resize(host.size()));
+  if (!host.empty())
+    DSS_CUDA(cudaMemcpyAsync(buf.ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return DSS_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+void dss_default_opts(dss_opts* o) {
+  if (!o) return;
+  o->device = 0;
+  o->schwarz_threshold = 1e-12;
+  o->boys_mode = DSS_BOYS_REF;
+}
+
+int dss_create(dss_ctx** out, const dss_opts* opts) {
+  if (!out) {
+    g_create_error = "dss_create: ctx pointer is NULL";
+    return DSS_ERR_INVALID;
+  }
+  *out = nullptr;
+  dss_ctx* ctx = new (std::nothrow) dss_ctx();
+  if (!ctx) {
+    g_create_error = "dss_create: out of host memory";
+    return DSS_ERR_OOM;
+  }
+  if (opts) ctx->opts = *opts;
+  else dss_default_opts(&ctx->opts);
+  if (ctx->opts.boys_mode != DSS_BOYS_REF && ctx->opts.boys_mode != DSS_BOYS_FAST) {
+    g_create_error = "dss_create: boys_mode must be DSS_BOYS_REF or DSS_BOYS_FAST";
+    delete ctx;
+    return DSS_ERR_INVALID;
+  }
+  if (!(ctx->opts.schwarz_threshold >= 0.0)) {
+    g_create_error = "dss_create: schwarz_threshold must be >= 0";
+    delete ctx;
+    return DSS_ERR_INVALID;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    g_create_error = std::string("dss_create: no CUDA device: ") + cudaGetErrorString(e);
+    delete ctx;
+    return DSS_ERR_CUDA;
+  }
+  if (ctx->opts.device < 0 || ctx->opts.device >= ndev) {
+    g_create_error = "dss_create: device ordinal out of range";
+    delete ctx;
+    return DSS_ERR_INVALID;
+  }
+  e = cudaSetDevice(ctx->opts.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  ctx->stream = ctx->own_stream;
+  if (e != cudaSuccess) {
+    g_create_error = std::string("dss_create: ") + cudaGetErrorString(e);
+    delete ctx;
+    return DSS_ERR_CUDA;
+  }
+  *out = ctx;
+  return DSS_OK;
+}
+
+void dss_destroy(dss_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->opts.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->release();
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+const char* dss_last_error(const dss_ctx* ctx) {
+  if (!ctx) return g_create_error.c_str();
+  return ctx->err.c_str();
+}
+
+int dss_nbf(const dss_ctx* ctx) { return ctx ? ctx->nbf : 0; }
+
+int dss_sync(dss_ctx* ctx) {
+  if (!ctx) return DSS_ERR_INVALID;
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  DSS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return DSS_OK;
+}
+
+int dss_set_basis(dss_ctx* ctx, int n_shell, const int* l, const int* nprim, const double* exps,
+                  const double* coefs, const double* centers, int pure) {
+  if (!ctx) return DSS_ERR_INVALID;
+  ctx->err.clear();
+  if (n_shell <= 0 || !l || !nprim || !exps || !coefs || !centers)
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_set_basis: empty basis or NULL array");
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  BasisHost B;
+  B.pure = pure ? 1 : 0;
+  int off = 0, f0 = 0;
+  for (int s = 0; s < n_shell; ++s) {
+    if (l[s] < 0 || l[s] > DSS_GEN_LMAX)
+      return dss_fail(ctx, DSS_ERR_UNSUPPORTED,
+                      "dss_set_basis: angular momentum " + std::to_string(l[s]) + " above the compiled maximum " +
+                          std::to_string(DSS_GEN_LMAX));
+    if (nprim[s] < 1 || nprim[s] > 100)
+      return dss_fail(ctx, DSS_ERR_INVALID,
+                      "dss_set_basis: Specified number of primitives (" + std::to_string(nprim[s]) +
+                          ") is outside of the accepted range of 1-100.");
+    B.l.push_back(l[s]);
+    B.nprim.push_back(nprim[s]);
+    B.prim0.push_back(off);
+    B.f0.push_back(f0);
+    for (int k = 0; k < 3; ++k) B.xyz.push_back(centers[3 * s + k]);
+    for (int p = 0; p < nprim[s]; ++p) {
+      const double zeta = exps[off + p];
+      if (!(zeta > 0.0)) return dss_fail(ctx, DSS_ERR_INVALID, "dss_set_basis: Primitive GTOs must have positive exponents!");
+      // chem/GTO.cpp:90-93, same operation order.
+      const double nf = (std::pow(2.0 * zeta, (double)l[s] + 1.5) * std::pow(2.0, (double)l[s] + 2)) /
+                        (std::sqrt(kPiRef) * dfact(2 * l[s] + 1));
+      B.exps.push_back(zeta);
+      B.wts.push_back(coefs[off + p] * std::sqrt(nf));
+    }
+    off += nprim[s];
+    f0 += pure ? 2 * l[s] + 1 : (l[s] + 1) * (l[s] + 2) / 2;
+  }
+  B.nbf = f0;
+  int rc = dss_setup_pairs(ctx, std::move(B));
+  if (rc != DSS_OK) return rc;
+  return DSS_OK;
+}
+
+int dss_work_stats(const dss_ctx* ctx, long long* sq, long long* pq, long long* wt) {
+  if (!ctx) return DSS_ERR_INVALID;
+  if (sq) *sq = ctx->n_shell_quartets;
+  if (pq) *pq = ctx->n_prim_quartets;
+  if (wt) *wt = ctx->n_warp_tasks;
+  return DSS_OK;
+}
+
+int dss_build_jk_device(dss_ctx* ctx, const double* D, double* J, double* K) {
+  if (!ctx) return DSS_ERR_INVALID;
+  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk_device: no basis set");
+  if (!D) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk_device: D is NULL");
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  const int n = ctx->nbf;
+  const size_t nn = (size_t)n * n;
+  DSS_CUDA(ctx->Jacc.resize(nn));
+  DSS_CUDA(ctx->Kacc.resize(nn));
+  int rc = dss_enqueue_jk(ctx, D, ctx->Jacc.ptr, ctx->Kacc.ptr);
+  if (rc != DSS_OK) return rc;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((nn + threads - 1) / threads);
+  if (J) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Jacc.ptr, J, nullptr, n);
+  if (K) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Kacc.ptr, K, nullptr, n);
+  DSS_CUDA(cudaGetLastError());
+  return DSS_OK;
+}
+
+int dss_build_jk(dss_ctx* ctx, const double* Dp, double* Jp, double* Kp) {
+  if (!ctx) return DSS_ERR_INVALID;
+  ctx->err.clear();
+  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk: no basis set (call dss_set_basis first)");
+  if (!Dp) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk: D is NULL");
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  const int n = ctx->nbf;
+  const size_t np = (size_t)n * (n + 1) / 2, nn = (size_t)n * n;
+  DSS_CUDA(ctx->packed_in.resize(np));
+  DSS_CUDA(ctx->packed_j.resize(np));
+  DSS_CUDA(ctx->packed_k.resize(np));
+  DSS_CUDA(ctx->Ddense.resize(nn));
+  DSS_CUDA(ctx->Jacc.resize(nn));
+  DSS_CUDA(ctx->Kacc.resize(nn));
+  DSS_CUDA(cudaMemcpyAsync(ctx->packed_in.ptr, Dp, np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((nn + threads - 1) / threads);
+  unpack_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->packed_in.ptr, ctx->Ddense.ptr, n);
+  DSS_CUDA(cudaGetLastError());
+  int rc = dss_enqueue_jk(ctx, ctx->Ddense.ptr, ctx->Jacc.ptr, ctx->Kacc.ptr);
+  if (rc != DSS_OK) return rc;
+  if (Jp) {
+    symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Jacc.ptr, nullptr, ctx->packed_j.ptr, n);
+    DSS_CUDA(cudaMemcpyAsync(Jp, ctx->packed_j.ptr, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (Kp) {
+    symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Kacc.ptr, nullptr, ctx->packed_k.ptr, n);
+    DSS_CUDA(cudaMemcpyAsync(Kp, ctx->packed_k.ptr, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  DSS_CUDA(cudaGetLastError());
+  DSS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return DSS_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ pairs, Schwarz, tasks
+int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
+  const int ns = (int)B.l.size();
+  // Unordered shell pairs {a, b}; stored with l_a >= l_b (ties: a >= b).
+  struct PairTmp {
+    int a, b, cls, npp;
+  };
+  std::vector<PairTmp> pairs;
+  pairs.reserve((size_t)ns * (ns + 1) / 2);
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j <= i; ++j) {
+      int a = i, b = j;
+      if (B.l[j] > B.l[i]) std::swap(a, b);
+      pairs.push_back({a, b, pair_class_index(B.l[a], B.l[b]), B.nprim[a] * B.nprim[b]});
+    }
+  // Order by class, then primitive-pair count (descending), then original order.
+  std::stable_sort(pairs.begin(), pairs.end(), [](const PairTmp& x, const PairTmp& y) {
+    if (x.cls != y.cls) return x.cls < y.cls;
+    return x.npp > y.npp;
+  });
+  const int np = (int)pairs.size();
+  std::vector<PrimPair> pp;
+  std::vector<int> pa(np), pb(np), p0(np), pn(np);
+  for (int q = 0; q < np; ++q) {
+    const int a = pairs[q].a, b = pairs[q].b;
+    pa[q] = a;
+    pb[q] = b;
+    p0[q] = (int)pp.size();
+    pn[q] = pairs[q].npp;
+    const double Ax = B.xyz[3 * a], Ay = B.xyz[3 * a + 1], Az = B.xyz[3 * a + 2];
+    const double Bx = B.xyz[3 * b], By = B.xyz[3 * b + 1], Bz = B.xyz[3 * b + 2];
+    const double ab2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+    for (int i = 0; i < B.nprim[a]; ++i)
+      for (int j = 0; j < B.nprim[b]; ++j) {
+        const double al = B.exps[B.prim0[a] + i], be = B.exps[B.prim0[b] + j];
+        const double p = al + be;
+        PrimPair r;
+        r.p = p;
+        r.inv_p = 1.0 / p;
+        r.Px = (al * Ax + be * Bx) / p;
+        r.Py = (al * Ay + be * By) / p;
+        r.Pz = (al * Az + be * Bz) / p;
+        r.PAx = r.Px - Ax;
+        r.PAy = r.Py - Ay;
+        r.PAz = r.Pz - Az;
+        // chem/GaussianIntegral.cpp:583,585: exp(-alpha*beta/eta * |A-B|^2) times the weights.
+        r.K = B.wts[B.prim0[a] + i] * B.wts[B.prim0[b] + j] * std::exp(-al * be / p * ab2);
+        r.pad = 0.0;
+        pp.push_back(r);
+      }
+  }
+  ctx->release_basis();
+  ctx->nbf = B.nbf;
+  ctx->pure = B.pure;
+  ctx->nshell = ns;
+  int rc;
+  if ((rc = upload(ctx, ctx->d_pp, pp)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_a, pa)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_b, pb)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_pp0, p0)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_npp, pn)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_sh_xyz, B.xyz)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_sh_f0, B.f0)) != DSS_OK) return rc;
+  DSS_CUDA(ctx->d_Q.resize(np));
+
+  // Class ranges.
+  const int ncls = DSS_N_PAIR_CLASSES;
+  std::vector<int> c0(ncls, 0), c1(ncls, 0);
+  for (int c = 0, q = 0; c < ncls; ++c) {
+    c0[c] = q;
+    while (q < np && pairs[q].cls == c) ++q;
+    c1[c] = q;
+  }
+  // Schwarz factors on the device, one launch per pair class.
+  for (int la = 0; la <= DSS_GEN_LMAX; ++la)
+    for (int lb = 0; lb <= la; ++lb) {
+      const int c = pair_class_index(la, lb);
+      if (c1[c] == c0[c]) continue;
+      SchwarzArgs sa;
+      sa.pair0 = c0[c];
+      sa.npair = c1[c] - c0[c];
+      sa.pair_a = ctx->d_pair_a.ptr;
+      sa.pair_b = ctx->d_pair_b.ptr;
+      sa.pair_pp0 = ctx->d_pair_pp0.ptr;
+      sa.pair_npp = ctx->d_pair_npp.ptr;
+      sa.pp = ctx->d_pp.ptr;
+      sa.sh_xyz = ctx->d_sh_xyz.ptr;
+      sa.Q = ctx->d_Q.ptr;
+      dss_launch_schwarz(la, lb, ctx->opts.boys_mode, ctx->pure, sa, ctx->stream);
+      DSS_CUDA(cudaGetLastError());
+    }
+  std::vector<double> Q(np);
+  DSS_CUDA(cudaMemcpyAsync(Q.data(), ctx->d_Q.ptr, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  DSS_CUDA(cudaStreamSynchronize(ctx->stream));
+
+  // Within each (class, npp) group: Schwarz factor descending.
+  std::vector<int> perm(np);
+  for (int q = 0; q < np; ++q) perm[q] = q;
+  std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) {
+    if (pairs[x].cls != pairs[y].cls) return pairs[x].cls < pairs[y].cls;
+    if (pairs[x].npp != pairs[y].npp) return pairs[x].npp > pairs[y].npp;
+    return Q[x] > Q[y];
+  });
+  std::vector<int> pa2(np), pb2(np), p02(np), pn2(np), cls2(np);
+  std::vector<double> Q2(np);
+  for (int q = 0; q < np; ++q) {
+    const int o = perm[q];
+    pa2[q] = pa[o];
+    pb2[q] = pb[o];
+    p02[q] = p0[o];
+    pn2[q] = pn[o];
+    cls2[q] = pairs[o].cls;
+    Q2[q] = Q[o];
+  }
+  if ((rc = upload(ctx, ctx->d_pair_a, pa2)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_b, pb2)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_pp0, p02)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_npp, pn2)) != DSS_OK) return rc;
+  ctx->h_pair_a = pa2;
+  ctx->h_pair_b = pb2;
+  ctx->h_pair_npp = pn2;
+  ctx->h_pair_cls = cls2;
+  ctx->h_Q = Q2;
+  ctx->class_pair0 = c0;
+  ctx->class_pair1 = c1;
+  return dss_build_tasks(ctx);
+}
+
+int dss_build_tasks(dss_ctx* ctx) {
+  const int ncls = DSS_N_PAIR_CLASSES;
+  const double thr = ctx->opts.schwarz_threshold;
+  const std::vector<double>& Q = ctx->h_Q;
+  const std::vector<int>& npp = ctx->h_pair_npp;
+  // npp groups per class: [g0, g1) ranges with equal npp.
+  std::vector<std::vector<std::pair<int, int>>> groups(ncls);
+  for (int c = 0; c < ncls; ++c) {
+    int q = ctx->class_pair0[c];
+    while (q < ctx->class_pair1[c]) {
+      int e = q;
+      while (e < ctx->class_pair1[c] && npp[e] == npp[q]) ++e;
+      groups[c].push_back({q, e});
+      q = e;
+    }
+  }
+  ctx->tasks.clear();
+  ctx->n_shell_quartets = 0;
+  ctx->n_prim_quartets = 0;
+  ctx->n_warp_tasks = 0;
+  struct ClassInfo {
+    int la, lb, lc, ld, bc, kc;
+  };
+  static const ClassInfo kClasses[] = {
+#define DSS_CLASS_ROW(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_, e_, f_},
+      DSS_FOR_EACH_CLASS(DSS_CLASS_ROW)
+#undef DSS_CLASS_ROW
+  };
+  for (const ClassInfo& ci : kClasses) {
+    const int bc = ci.bc, kc = ci.kc;
+    ClassTasks ct;
+    ct.la = ci.la;
+    ct.lb = ci.lb;
+    ct.lc = ci.lc;
+    ct.ld = ci.ld;
+    std::vector<int4> h;
+    for (int ib = ctx->class_pair0[bc]; ib < ctx->class_pair1[bc]; ++ib) {
+      const double Qb = Q[ib];
+      for (const auto& g : groups[kc]) {
+        int hi = g.second;
+        if (bc == kc) hi = std::min(hi, ib + 1);
+        if (hi <= g.first) continue;
+        // Q is descending in [g.first, hi): count the kets with Qb * Qk >= thr.
+        int lo_i = g.first, hi_i = hi;
+        while (lo_i < hi_i) {
+          const int mid = (lo_i + hi_i) / 2;
+          if (Qb * Q[mid] >= thr) lo_i = mid + 1;
+          else hi_i = mid;
+        }
+        const int nvalid = lo_i - g.first;
+        for (int k0 = 0; k0 < nvalid; k0 += 32) {
+          const int cnt = std::min(32, nvalid - k0);
+          h.push_back(make_int4(ib, g.first + k0, cnt, 0));
+          ct.shell_quartets += cnt;
+          ct.prim_quartets += (long long)cnt * npp[ib] * npp[g.first];
+        }
+      }
+    }
+    ct.ntasks = (int)h.size();
+    ctx->n_warp_tasks += ct.ntasks;
+    ctx->n_shell_quartets += ct.shell_quartets;
+    ctx->n_prim_quartets += ct.prim_quartets;
+    ctx->tasks.push_back(std::move(ct));
+    int rc_ = upload(ctx, ctx->tasks.back().d_tasks, h);
+    if (rc_ != DSS_OK) return rc_;
+  }
+  DSS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return DSS_OK;
+}
+
+int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events) {
+  const int n = ctx->nbf;
+  const size_t nn = (size_t)n * n;
+  DSS_CUDA(cudaMemsetAsync(Jacc, 0, nn * sizeof(double), ctx->stream));
+  DSS_CUDA(cudaMemsetAsync(Kacc, 0, nn * sizeof(double), ctx->stream));
+  for (size_t ci = 0; ci < ctx->tasks.size(); ++ci) {
+    ClassTasks& ct = ctx->tasks[ci];
+    if (!ct.ntasks) continue;
+    EriArgs a;
+    a.tasks = ct.d_tasks.ptr;
+    a.ntasks = ct.ntasks;
+    a.pair_a = ctx->d_pair_a.ptr;
+    a.pair_b = ctx->d_pair_b.ptr;
+    a.pair_pp0 = ctx->d_pair_pp0.ptr;
+    a.pair_npp = ctx->d_pair_npp.ptr;
+    a.pp = ctx->d_pp.ptr;
+    a.sh_xyz = ctx->d_sh_xyz.ptr;
+    a.sh_f0 = ctx->d_sh_f0.ptr;
+    a.D = D;
+    a.J = Jacc;
+    a.K = Kacc;
+    a.n = n;
+    if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], ctx->stream));
+    dss_launch_eri_jk(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, a, ctx->stream);
+    DSS_CUDA(cudaGetLastError());
+    if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], ctx->stream));
+  }
+  return DSS_OK;
+}
+
+namespace {
+// FP64 FMA throughput probe: 8 independent register chains per thread.
+__global__ void fp64_probe_kernel(double* out, int iters, double b, double c) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-10, a2 = a0 + 2e-10, a3 = a0 + 3e-10;
+  double a4 = a0 + 4e-10, a5 = a0 + 5e-10, a6 = a0 + 6e-10, a7 = a0 + 7e-10;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+    a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+  }
+  const double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 1234.5678) out[0] = r;  // never true; keeps the chains alive
+}
+}  // namespace
+
+extern "C" {
+
+int dss_set_stream(dss_ctx* ctx, void* stream) {
+  if (!ctx) return DSS_ERR_INVALID;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return DSS_OK;
+}
+
+void* dss_get_stream(const dss_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int dss_num_classes(void) { return DSS_N_QUARTET_CLASSES; }
+
+int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* sq, long long* pq, long long* wt) {
+  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES) return DSS_ERR_INVALID;
+  static const int kL[][4] = {
+#define DSS_CLASS_L(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_},
+      DSS_FOR_EACH_CLASS(DSS_CLASS_L)
+#undef DSS_CLASS_L
+  };
+  if (l4)
+    for (int k = 0; k < 4; ++k) l4[k] = kL[i][k];
+  const bool have = (size_t)i < ctx->tasks.size();
+  if (sq) *sq = have ? ctx->tasks[i].shell_quartets : 0;
+  if (pq) *pq = have ? ctx->tasks[i].prim_quartets : 0;
+  if (wt) *wt = have ? ctx->tasks[i].ntasks : 0;
+  return DSS_OK;
+}
+
+int dss_kernels_per_build(const dss_ctx* ctx) {
+  if (!ctx) return 0;
+  int k = 0;
+  for (const auto& ct : ctx->tasks)
+    if (ct.ntasks) ++k;
+  return k + 2;  // + the two symmetrisations
+}
+
+int dss_profile_build(dss_ctx* ctx, const double* D, double* J, double* K, float* ms) {
+  if (!ctx || !ms) return DSS_ERR_INVALID;
+  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_profile_build: no basis set");
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  const int nc = (int)ctx->tasks.size();
+  std::vector<cudaEvent_t> ev(2 * nc);
+  for (auto& e : ev) DSS_CUDA(cudaEventCreate(&e));
+  const int n = ctx->nbf;
+  const size_t nn = (size_t)n * n;
+  int rc = DSS_OK;
+  if (ctx->Jacc.resize(nn) != cudaSuccess || ctx->Kacc.resize(nn) != cudaSuccess)
+    rc = dss_fail(ctx, DSS_ERR_OOM, "dss_profile_build: device allocation failed");
+  if (rc == DSS_OK) rc = dss_enqueue_jk(ctx, D, ctx->Jacc.ptr, ctx->Kacc.ptr, ev.data());
+  if (rc == DSS_OK) {
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((nn + threads - 1) / threads);
+    if (J) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Jacc.ptr, J, nullptr, n);
+    if (K) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Kacc.ptr, K, nullptr, n);
+    rc = dss_cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "dss_profile_build");
+  }
+  for (int i = 0; i < DSS_N_QUARTET_CLASSES; ++i) ms[i] = 0.0f;
+  if (rc == DSS_OK)
+    for (int i = 0; i < nc; ++i)
+      if (ctx->tasks[i].ntasks) cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+  for (auto& e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
+int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops) {
+  if (!ctx || !tflops) return DSS_ERR_INVALID;
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  int nsm = 0;
+  DSS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->opts.device));
+  DevBuf<double> out;
+  DSS_CUDA(out.resize(1));
+  const int threads = 256, blocks = nsm * 8, iters = 1 << 14;
+  cudaEvent_t e0, e1;
+  DSS_CUDA(cudaEventCreate(&e0));
+  DSS_CUDA(cudaEventCreate(&e1));
+  fp64_probe_kernel<<<blocks, threads, 0, ctx->stream>>>(out.ptr, iters, 0.999999, 1e-7);  // warm-up
+  DSS_CUDA(cudaEventRecord(e0, ctx->stream));
+  fp64_probe_kernel<<<blocks, threads, 0, ctx->stream>>>(out.ptr, iters, 0.999999, 1e-7);
+  DSS_CUDA(cudaEventRecord(e1, ctx->stream));
+  DSS_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.0f;
+  DSS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *tflops = 2.0 * 8.0 * (double)iters * threads * blocks / (ms * 1e-3) / 1e12;
+  return DSS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// Internal state of a dss_ctx (the C ABI's opaque handle).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "dss.h"
+
+struct PrimPair;
+
+// Device buffer that grows on demand and frees on destruction.
+template <class T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), n(o.n) {
+    o.ptr = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      free();
+      ptr = o.ptr;
+      n = o.n;
+      o.ptr = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { free(); }
+  cudaError_t resize(size_t count) {
+    if (count <= n && ptr) return cudaSuccess;
+    free();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void**)&ptr, count * sizeof(T));
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      n = 0;
+      return e;
+    }
+    n = count;
+    return cudaSuccess;
+  }
+  void free() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+};
+
+struct BasisHost {
+  int pure = 1;
+  int nbf = 0;
+  std::vector<int> l, nprim, prim0, f0;
+  std::vector<double> xyz, exps, wts;
+};
+
+struct ClassTasks {
+  int la = 0, lb = 0, lc = 0, ld = 0;
+  int ntasks = 0;
+  long long shell_quartets = 0, prim_quartets = 0;
+  DevBuf<int4> d_tasks;
+};
+
+struct dss_ctx {
+  dss_opts opts{};
+  cudaStream_t stream = nullptr;      // the stream work is enqueued on
+  cudaStream_t own_stream = nullptr;  // created with the context
+  std::string err;
+
+  // basis
+  int nbf = 0, pure = 1, nshell = 0;
+  DevBuf<PrimPair> d_pp;
+  DevBuf<int> d_pair_a, d_pair_b, d_pair_pp0, d_pair_npp, d_sh_f0;
+  DevBuf<double> d_sh_xyz, d_Q;
+  std::vector<int> h_pair_a, h_pair_b, h_pair_npp, h_pair_cls;
+  std::vector<double> h_Q;
+  std::vector<int> class_pair0, class_pair1;
+  std::vector<ClassTasks> tasks;
+  long long n_shell_quartets = 0, n_prim_quartets = 0, n_warp_tasks = 0;
+
+  // build scratch
+  DevBuf<double> packed_in, packed_j, packed_k, Ddense, Jacc, Kacc;
+
+  void release_basis() {
+    d_pp.free();
+    d_pair_a.free();
+    d_pair_b.free();
+    d_pair_pp0.free();
+    d_pair_npp.free();
+    d_sh_f0.free();
+    d_sh_xyz.free();
+    d_Q.free();
+    tasks.clear();
+    nbf = 0;
+  }
+  void release() {
+    release_basis();
+    packed_in.free();
+    packed_j.free();
+    packed_k.free();
+    Ddense.free();
+    Jacc.free();
+    Kacc.free();
+  }
+};
+
+int dss_fail(dss_ctx* ctx, int code, const std::string& msg);
+int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what);
+int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
+int dss_build_tasks(dss_ctx* ctx);
+// Enqueues one J/K accumulation; with events != NULL records events[2i], events[2i+1]
+// around the launch of class i.
+int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events = nullptr);

@@ -1,0 +1,229 @@
+// ERI + J/K digest kernels and the Schwarz diagonal kernel, templated on the
+// shell-quartet class.  The per-class integral code comes from eri_gen.cuh.
+//
+// Work decomposition: a warp owns one bra shell pair (ab) and up to 32 ket shell
+// pairs (cd), one per lane (a "warp task").  Ket pairs of a task are consecutive
+// in the class's pair list, which is sorted by primitive-pair count and then by
+// Schwarz bound, so all lanes of a warp run the same primitive loop trip counts.
+//
+// Digest (the J/K of chem/scf/ExactCoulomb.cpp:103-123 over the 8-fold unique
+// quartets of :54-68): for a unique shell quartet every function quartet
+// (ij|kl) is scaled by s = 1/2 per coincidence (a == b, c == d, ab == cd) and
+// contributes
+//   Jacc[i][j] += 2 s (ij|kl) D[k][l],   Jacc[k][l] += 2 s (ij|kl) D[i][j],
+//   Kacc[i][l] += s (ij|kl) D[j][k],     Kacc[j][l] += s (ij|kl) D[i][k],
+//   Kacc[i][k] += s (ij|kl) D[j][l],     Kacc[j][k] += s (ij|kl) D[i][l],
+// and finally J = Jacc + Jacc^T, K = Kacc + Kacc^T, so that
+//   J[m][n] = sum_st D[s][t] (mn|st),   K[m][n] = sum_st D[s][t] (mt|sn).
+// Each thread first sums its quartet's contributions per target element; the
+// Jacc[i][j] sums, shared by the whole warp (same bra pair), are reduced with
+// warp shuffles before a single atomic per element.
+#pragma once
+#include "common.cuh"
+#include "eri_gen.cuh"
+
+struct EriArgs {
+  const int4* tasks;      // {bra pair, first ket pair, ket count, 0}
+  int ntasks;
+  const int* pair_a;      // shell index of a (pair order: l_a >= l_b)
+  const int* pair_b;
+  const int* pair_pp0;    // first primitive pair
+  const int* pair_npp;    // primitive pairs in the pair
+  const PrimPair* pp;
+  const double* sh_xyz;   // [nshell][3] bohr
+  const int* sh_f0;       // first basis function of each shell
+  const double* D;        // dense n x n density (row-major, symmetric)
+  double* J;              // dense n x n accumulators (Jacc, Kacc above)
+  double* K;
+  int n;
+};
+
+struct SchwarzArgs {
+  int pair0, npair;       // pair range of one pair class
+  const int* pair_a;
+  const int* pair_b;
+  const int* pair_pp0;
+  const int* pair_npp;
+  const PrimPair* pp;
+  const double* sh_xyz;
+  double* Q;              // out: sqrt(max |(ij|ij)|) per pair
+};
+
+__host__ __device__ constexpr int dss_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int dss_nfunc(int l, bool pure) { return pure ? 2 * l + 1 : dss_ncart(l); }
+
+template <int LA, int LB, int LC, int LD>
+struct EriClass;
+
+#define DSS_DEFINE_ERI_CLASS(la, lb, lc, ld, bc, kc)                                                    \
+  template <>                                                                                           \
+  struct EriClass<la, lb, lc, ld> {                                                                     \
+    template <int BOYS, bool PURE>                                                                      \
+    __device__ __forceinline__ static void eval(const PrimPair* bra, int nb, const PrimPair* ket, int nk, \
+                                                double ABx, double ABy, double ABz, double CDx,         \
+                                                double CDy, double CDz, double* I) {                    \
+      eri_##la##lb##lc##ld<BOYS, PURE>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I);             \
+    }                                                                                                   \
+  };
+DSS_FOR_EACH_CLASS(DSS_DEFINE_ERI_CLASS)
+#undef DSS_DEFINE_ERI_CLASS
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE>
+__global__ void __launch_bounds__(128) eri_jk_kernel(EriArgs a) {
+  constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
+  constexpr int NC = dss_nfunc(LC, PURE), ND = dss_nfunc(LD, PURE);
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (warp >= a.ntasks) return;  // uniform per warp
+  const int4 t = __ldg(a.tasks + warp);
+  const bool active = lane < t.z;
+  const int bra = t.x;
+  const int ket = t.y + (active ? lane : 0);
+  const int sa = __ldg(a.pair_a + bra), sb = __ldg(a.pair_b + bra);
+  const int sc = __ldg(a.pair_a + ket), sd = __ldg(a.pair_b + ket);
+  const double Ax = __ldg(a.sh_xyz + 3 * sa), Ay = __ldg(a.sh_xyz + 3 * sa + 1), Az = __ldg(a.sh_xyz + 3 * sa + 2);
+  const double Bx = __ldg(a.sh_xyz + 3 * sb), By = __ldg(a.sh_xyz + 3 * sb + 1), Bz = __ldg(a.sh_xyz + 3 * sb + 2);
+  const double Cx = __ldg(a.sh_xyz + 3 * sc), Cy = __ldg(a.sh_xyz + 3 * sc + 1), Cz = __ldg(a.sh_xyz + 3 * sc + 2);
+  const double Dx = __ldg(a.sh_xyz + 3 * sd), Dy = __ldg(a.sh_xyz + 3 * sd + 1), Dz = __ldg(a.sh_xyz + 3 * sd + 2);
+
+  double I[NA * NB * NC * ND];
+  if (active) {
+    EriClass<LA, LB, LC, LD>::template eval<BOYS, PURE>(
+        a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
+        __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, I);
+  } else {
+#pragma unroll
+    for (int q = 0; q < NA * NB * NC * ND; ++q) I[q] = 0.0;
+  }
+  double s = 1.0;
+  if (sa == sb) s *= 0.5;
+  if (sc == sd) s *= 0.5;
+  if (bra == ket) s *= 0.5;
+  const int n = a.n;
+  const int fa = __ldg(a.sh_f0 + sa), fb = __ldg(a.sh_f0 + sb);
+  const int fc = __ldg(a.sh_f0 + sc), fd = __ldg(a.sh_f0 + sd);
+  const double* __restrict__ D = a.D;
+
+  // Density blocks.
+  double dab[NA * NB], dcd[NC * ND], dad[NA * ND], dbd[NB * ND], dac[NA * NC], dbc[NB * NC];
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int j = 0; j < NB; ++j) dab[i * NB + j] = __ldg(D + (size_t)(fa + i) * n + fb + j);
+#pragma unroll
+  for (int k = 0; k < NC; ++k)
+#pragma unroll
+    for (int l = 0; l < ND; ++l) dcd[k * ND + l] = __ldg(D + (size_t)(fc + k) * n + fd + l);
+#pragma unroll
+  for (int i = 0; i < NA; ++i) {
+#pragma unroll
+    for (int l = 0; l < ND; ++l) dad[i * ND + l] = __ldg(D + (size_t)(fa + i) * n + fd + l);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) dac[i * NC + k] = __ldg(D + (size_t)(fa + i) * n + fc + k);
+  }
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+#pragma unroll
+    for (int l = 0; l < ND; ++l) dbd[j * ND + l] = __ldg(D + (size_t)(fb + j) * n + fd + l);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) dbc[j * NC + k] = __ldg(D + (size_t)(fb + j) * n + fc + k);
+  }
+
+  double jab[NA * NB], jcd[NC * ND], kad[NA * ND], kbd[NB * ND], kac[NA * NC], kbc[NB * NC];
+#pragma unroll
+  for (int q = 0; q < NA * NB; ++q) jab[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < NC * ND; ++q) jcd[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < NA * ND; ++q) kad[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < NB * ND; ++q) kbd[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < NA * NC; ++q) kac[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < NB * NC; ++q) kbc[q] = 0.0;
+
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) {
+          const double v = s * I[((i * NB + j) * NC + k) * ND + l];
+          jab[i * NB + j] += v * dcd[k * ND + l];
+          jcd[k * ND + l] += v * dab[i * NB + j];
+          kad[i * ND + l] += v * dbc[j * NC + k];
+          kbd[j * ND + l] += v * dac[i * NC + k];
+          kac[i * NC + k] += v * dbd[j * ND + l];
+          kbc[j * NC + k] += v * dad[i * ND + l];
+        }
+
+  // Bra-pair J block: same target for the whole warp.
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const double v = warp_sum(jab[i * NB + j]);
+      if (lane == 0) atomicAdd(a.J + (size_t)(fa + i) * n + fb + j, 2.0 * v);
+    }
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) atomicAdd(a.J + (size_t)(fc + k) * n + fd + l, 2.0 * jcd[k * ND + l]);
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+#pragma unroll
+      for (int l = 0; l < ND; ++l) atomicAdd(a.K + (size_t)(fa + i) * n + fd + l, kad[i * ND + l]);
+#pragma unroll
+      for (int k = 0; k < NC; ++k) atomicAdd(a.K + (size_t)(fa + i) * n + fc + k, kac[i * NC + k]);
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+#pragma unroll
+      for (int l = 0; l < ND; ++l) atomicAdd(a.K + (size_t)(fb + j) * n + fd + l, kbd[j * ND + l]);
+#pragma unroll
+      for (int k = 0; k < NC; ++k) atomicAdd(a.K + (size_t)(fb + j) * n + fc + k, kbc[j * NC + k]);
+    }
+  }
+}
+
+// Schwarz factors Q_ab = sqrt(max_ij |(ij|ij)|) for the pairs of one class.
+template <int LA, int LB, int BOYS, bool PURE>
+__global__ void __launch_bounds__(128) schwarz_kernel(SchwarzArgs a) {
+  constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.npair) return;
+  const int pr = a.pair0 + idx;
+  const int sa = a.pair_a[pr], sb = a.pair_b[pr];
+  const double ABx = a.sh_xyz[3 * sa] - a.sh_xyz[3 * sb];
+  const double ABy = a.sh_xyz[3 * sa + 1] - a.sh_xyz[3 * sb + 1];
+  const double ABz = a.sh_xyz[3 * sa + 2] - a.sh_xyz[3 * sb + 2];
+  const PrimPair* pp = a.pp + a.pair_pp0[pr];
+  const int npp = a.pair_npp[pr];
+  double I[NA * NB * NA * NB];
+  EriClass<LA, LB, LA, LB>::template eval<BOYS, PURE>(pp, npp, pp, npp, ABx, ABy, ABz, ABx, ABy, ABz, I);
+  double mx = 0.0;
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int j = 0; j < NB; ++j) mx = fmax(mx, fabs(I[((i * NB + j) * NA + i) * NB + j]));
+  a.Q[pr] = sqrt(mx);
+}
+
+// Host-side launchers (one translation unit per class defines them).
+#define DSS_DECLARE_LAUNCHERS(la, lb, lc, ld, bc, kc) \
+  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, const EriArgs& a, cudaStream_t s);
+DSS_FOR_EACH_CLASS(DSS_DECLARE_LAUNCHERS)
+#undef DSS_DECLARE_LAUNCHERS
+
+void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s);
+void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, const EriArgs& a, cudaStream_t s);

@@ -1,0 +1,136 @@
+"""Python mirror of the C ABI: the two-electron part of the reference's SCF.
+
+``FockBuilder`` plays the role of the reference's ExactCoulomb module
+(chem/scf/ExactCoulomb.hpp:9-15): ``set_basis`` replaces
+``assignExactRepulsionTensor`` (no stored tensor: integrals are recomputed on
+the GPU per build, "direct SCF"), ``jk`` returns the whole Coulomb and exchange
+matrices that ``getExactCoulombMatrix`` / ``getExactExchangeMatrix`` return
+element by element.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from .shells import ShellArrays
+
+BOYS_REF = 0
+BOYS_FAST = 1
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class FockBuilder:
+    def __init__(self, device: int = 0, schwarz_threshold: float = 1e-12, boys_mode: int = BOYS_REF):
+        self._L = _lib.load()
+        opts = _lib.DssOpts(device, schwarz_threshold, boys_mode)
+        h = ctypes.c_void_p()
+        rc = self._L.dss_create(ctypes.byref(h), ctypes.byref(opts))
+        if rc != 0:
+            raise _lib.DssError(rc, self._L.dss_last_error(None).decode())
+        self._h = h
+        self.nbf = 0
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise _lib.DssError(rc, self._L.dss_last_error(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.dss_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_basis(self, sh: ShellArrays) -> int:
+        l = np.ascontiguousarray(sh.shell_l, dtype=np.int32)
+        n = np.ascontiguousarray(sh.shell_nprim, dtype=np.int32)
+        e = np.ascontiguousarray(sh.exps, dtype=np.float64)
+        c = np.ascontiguousarray(sh.coefs, dtype=np.float64)
+        x = np.ascontiguousarray(sh.centers, dtype=np.float64).ravel()
+        self._check(self._L.dss_set_basis(self._h, sh.nshell, _ip(l), _ip(n), _dp(e), _dp(c), _dp(x),
+                                          1 if sh.pure else 0))
+        self.nbf = self._L.dss_nbf(self._h)
+        return self.nbf
+
+    def jk(self, D_packed: np.ndarray, want_j: bool = True, want_k: bool = True
+           ) -> Tuple[Optional[np.ndarray], Optional[np.ndarray]]:
+        n = self.nbf
+        np_ = n * (n + 1) // 2
+        D = np.ascontiguousarray(D_packed, dtype=np.float64)
+        if D.shape != (np_,):
+            raise ValueError(f"D must be packed-U with {np_} entries")
+        J = np.empty(np_) if want_j else None
+        K = np.empty(np_) if want_k else None
+        self._check(self._L.dss_build_jk(self._h, _dp(D), _dp(J) if J is not None else None,
+                                         _dp(K) if K is not None else None))
+        return J, K
+
+    def jk_device(self, D_ptr: int, J_ptr: int, K_ptr: int) -> None:
+        """Build on device-resident dense n x n buffers (raw device pointers)."""
+        self._check(self._L.dss_build_jk_device(self._h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(J_ptr),
+                                                ctypes.c_void_p(K_ptr)))
+
+    def jk_host_ptrs(self, D_ptr: int, J_ptr: int, K_ptr: int) -> None:
+        """dss_build_jk on raw host pointers (e.g. pinned buffers)."""
+        self._check(self._L.dss_build_jk(self._h, ctypes.cast(D_ptr, ctypes.POINTER(ctypes.c_double)),
+                                         ctypes.cast(J_ptr, ctypes.POINTER(ctypes.c_double)),
+                                         ctypes.cast(K_ptr, ctypes.POINTER(ctypes.c_double))))
+
+    def stream_ptr(self) -> int:
+        return int(self._L.dss_get_stream(self._h) or 0)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self._L.dss_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def class_info(self, i: int):
+        l4 = (ctypes.c_int * 4)()
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self._L.dss_class_info(self._h, i, l4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return list(l4), a.value, b.value, c.value
+
+    def kernels_per_build(self) -> int:
+        return int(self._L.dss_kernels_per_build(self._h))
+
+    def profile_build(self, D_ptr: int, J_ptr: int, K_ptr: int):
+        nc = self._L.dss_num_classes()
+        ms = (ctypes.c_float * nc)()
+        self._check(self._L.dss_profile_build(self._h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(J_ptr),
+                                              ctypes.c_void_p(K_ptr), ms))
+        return [float(v) for v in ms]
+
+    def fp64_peak_tflops(self) -> float:
+        t = ctypes.c_double()
+        self._check(self._L.dss_probe_fp64_peak(self._h, ctypes.byref(t)))
+        return t.value
+
+    def sync(self) -> None:
+        self._check(self._L.dss_sync(self._h))
+
+    def work_stats(self) -> Tuple[int, int, int]:
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self._L.dss_work_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value

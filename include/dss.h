@@ -1,0 +1,120 @@
+/*
+ * dss.h -- C ABI of the B200 Fock-build engine for DollarStoreSCF.
+ *
+ * All matrices crossing this boundary on the host are symmetric n x n matrices in
+ * the reference's packed-upper column-major layout (LAPACK 'U' packed): element
+ * (y <= x) lives at index x*(x+1)/2 + y (lalib/Matrix.ipp:332-356).  The caller
+ * owns every host array; no pointer is kept after a call returns.  Every call
+ * returns DSS_OK (0) or a negative status and records a message readable with
+ * dss_last_error(); nothing aborts the process.  One context per host thread.
+ *
+ * Function order matches scf::constructBasis (chem/scf/SCFBasis.cpp:120-139):
+ * shells in the order given, m = -l..l inside a spherical shell (the reference's
+ * real solid harmonics, chem/GTO.cpp:15-94); inside a Cartesian (6D) shell the
+ * monomials x^a y^b z^c are ordered a descending then b descending, each scaled
+ * to unit self-overlap.
+ */
+#ifndef DSS_H
+#define DSS_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSS_OK 0
+#define DSS_ERR_INVALID (-1)     /* bad argument or call order */
+#define DSS_ERR_OOM (-2)         /* device or host allocation failed */
+#define DSS_ERR_CUDA (-3)        /* CUDA runtime / launch error */
+#define DSS_ERR_NOCONV (-4)      /* SCF reached its iteration cap */
+#define DSS_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define DSS_ERR_UNSUPPORTED (-6) /* e.g. angular momentum above the compiled maximum */
+
+#define DSS_BOYS_REF 0  /* the reference's truncated series (parity mode) */
+#define DSS_BOYS_FAST 1 /* accurate tabulated Boys function */
+
+typedef struct dss_ctx dss_ctx;
+
+typedef struct dss_opts {
+  int device;               /* CUDA device ordinal */
+  double schwarz_threshold; /* drop shell quartets with Q_ab Q_cd below this (0: keep all) */
+  int boys_mode;            /* DSS_BOYS_REF or DSS_BOYS_FAST */
+} dss_opts;
+
+/* Defaults: device 0, Schwarz threshold 1e-12, reference Boys. */
+void dss_default_opts(dss_opts* opts);
+
+/* Creates a context on opts->device (opts may be NULL for the defaults).
+ * Replaces the reference's global two-electron state (chem/scf/ExactCoulomb.cpp:13-15). */
+int dss_create(dss_ctx** ctx, const dss_opts* opts);
+
+void dss_destroy(dss_ctx* ctx);
+
+/* Message of the last failed call on ctx ("" if none).  With ctx == NULL: the
+ * last dss_create failure. */
+const char* dss_last_error(const dss_ctx* ctx);
+
+/* Basis of one molecule as shells.  l[s], nprim[s]; exps/coefs concatenated in
+ * shell order; coefs are the basis file's contraction coefficients (the library
+ * applies the reference's primitive normalisation, chem/GTO.cpp:90-93, and no
+ * contraction renormalisation).  centers_bohr[3*s].  pure = 1: spherical (5D)
+ * functions as in the reference; pure = 0: Cartesian (6D).
+ * Computes Schwarz factors on the device and the screened quartet work lists.
+ * Replaces the set-up half of assignExactRepulsionTensor (ExactCoulomb.cpp:41-52). */
+int dss_set_basis(dss_ctx* ctx, int n_shell, const int* l, const int* nprim, const double* exps,
+                  const double* coefs, const double* centers_bohr, int pure);
+
+/* Number of basis functions of the current basis. */
+int dss_nbf(const dss_ctx* ctx);
+
+/* Coulomb and exchange matrices of one symmetric density D (packed-U, n(n+1)/2):
+ *   J[m][n] = sum_st D[s][t] (mn|st)      (getExactCoulombMatrix, ExactCoulomb.cpp:103-112)
+ *   K[m][n] = sum_st D[s][t] (mt|sn)      (getExactExchangeMatrix, ExactCoulomb.cpp:114-123)
+ * The reference's RHF two-electron Fock part G = J[D_total] - K[D_alpha]
+ * (SCFSolver.cpp:29-43) is J - K/2 of one call with D = D_total.
+ * Either output may be NULL.  Host arrays; returns after the results are copied back. */
+int dss_build_jk(dss_ctx* ctx, const double* D_packed, double* J_packed, double* K_packed);
+
+/* Same build on device-resident dense row-major n x n matrices (device
+ * pointers, symmetric D); enqueued on the context's stream, which the caller
+ * synchronises with dss_sync().  For callers that keep densities in HBM. */
+int dss_build_jk_device(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev);
+
+/* Waits for the context's stream. */
+int dss_sync(dss_ctx* ctx);
+
+/* Work statistics of the current basis: unique shell quartets kept by the
+ * Schwarz screen, primitive quartets they hold, and the warp tasks. */
+int dss_work_stats(const dss_ctx* ctx, long long* shell_quartets, long long* prim_quartets, long long* warp_tasks);
+
+/* Uses the caller's CUDA stream (a cudaStream_t passed as void*) for all
+ * later work on ctx; NULL restores the context's own stream. */
+int dss_set_stream(dss_ctx* ctx, void* stream);
+
+/* The stream ctx currently enqueues on (a cudaStream_t as void*). */
+void* dss_get_stream(const dss_ctx* ctx);
+
+/* Shell-quartet classes (la lb|lc ld) the library was compiled with. */
+int dss_num_classes(void);
+
+/* Class i: its angular momenta and, for the current basis, the screened shell
+ * and primitive quartets and warp tasks it holds. */
+int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* shell_quartets, long long* prim_quartets,
+                   long long* warp_tasks);
+
+/* Kernel launches one dss_build_jk_device call enqueues. */
+int dss_kernels_per_build(const dss_ctx* ctx);
+
+/* One dss_build_jk_device with a CUDA event pair around every class launch;
+ * ms_per_class[dss_num_classes()] receives each launch's device time (0 for
+ * classes without work).  Synchronises the stream. */
+int dss_profile_build(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev,
+                      float* ms_per_class);
+
+/* Measures the device's double-precision FMA throughput with a register-only
+ * loop (the FP64 CUDA-core roofline the ERI kernels are reported against). */
+int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSS_H */

@@ -41,17 +41,19 @@ static double ref_ipow(double x, unsigned p) {
   return y * ref_ipow(x, p - l / 2);
 }
 
-static double dfact(int n) {
-  double r = 1.0;
-  for (int i = n; i > 0; i -= 2) r *= i;
-  return r;
+/* (2m-1)!! as the reference evaluates it: in 32-bit int arithmetic
+ * (doubleFactorial<int>, lalib/MathUtil.hpp:36-42), which wraps for m >= 11. */
+static double dfact_int32(int n) {
+  unsigned int r = 1u;
+  for (int i = n; i > 0; i -= 2) r *= (unsigned int)i;
+  return (double)(int)r;
 }
 
 double orc_boys_ref(double x, unsigned m) {
   if (x > (double)m * 1.1 + 25.0) {
     double pw2 = 1.0;
     for (unsigned i = 0; i < m + 1; ++i) pw2 *= 2.0;
-    return dfact(2 * (int)m - 1) / pw2 * sqrt(ORC_PI / ref_ipow(x, 2 * m + 1));
+    return dfact_int32(2 * (int)m - 1) / pw2 * sqrt(ORC_PI / ref_ipow(x, 2 * m + 1));
   }
   double F = 1.0, a = 1.0;
   for (int i = 1; a > 0.000000001; ++i) {

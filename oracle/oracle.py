@@ -30,6 +30,7 @@ import subprocess
 from typing import Dict, List, Tuple
 
 import numpy as np
+from scipy.linalg import lapack
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SO_PATH = os.path.join(HERE, "liboracle.so")
@@ -249,7 +250,12 @@ def scf_rhf(S: np.ndarray, H: np.ndarray, eri: np.ndarray, n_alpha: int, e_nuc: 
                 M[:cnt, cnt] = M[cnt, :cnt] = 1.0
                 rhs = np.zeros(cnt + 1)
                 rhs[cnt] = 1.0
-                c = np.linalg.solve(M, rhs)
+                # dspsv (lalib/Lapack.cpp:145-170): Bunch-Kaufman LDL^T.  When D is
+                # exactly singular LAPACK reports info > 0, skips the solve and the
+                # reference keeps the right-hand side as the coefficients.
+                _, _, c, info = lapack.dsysv(M, rhs, lower=0)
+                if info > 0:
+                    c = rhs
                 F = sum(c[i] * focks[i] for i in range(cnt))
         eps, Cp = np.linalg.eigh(X @ F @ X)
         C = X @ Cp

@@ -1,0 +1,130 @@
+"""Host-side logic: loaders, geometry generators, packed layout, shells."""
+import os
+
+import numpy as np
+import pytest
+
+from dollarstorescf_b200 import basis, geometry, shells
+
+SAMPLE = """\
+! comment
+H     0
+S    3   1.00
+      0.1873113696D+02       0.3349460434D-01
+      0.2825394365D+01       0.2347269535D+00
+      0.6401216923D+00       0.8137573261D+00
+S    1   1.00
+      0.1612777588D+00       1.0000000
+****
+C     0
+S    1   1.00
+      0.3047524880D+01       1.0
+SP   2   1.00
+      0.2324918408D+01      -0.3509174574D-01       0.8941508043D-02
+      0.6324303556D+00      -0.1912328431D+00       0.1410094640D+00
+D    1   1.00
+      0.8000000000D+00       1.0000000
+****
+"""
+
+
+def test_parse_basis_sp_split_and_d_exponents():
+    bs = basis.parse_basis_text(SAMPLE)
+    assert [s.l for s in bs.elements[1]] == [0, 0]
+    assert bs.elements[1][0].exps[0] == pytest.approx(18.73113696)
+    c = bs.elements[6]
+    assert [s.l for s in c] == [0, 0, 1, 2]
+    assert c[1].exps == c[2].exps
+    assert c[2].coefs[1] == pytest.approx(0.1410094640)
+
+
+def test_parse_basis_errors():
+    with pytest.raises(basis.BasisError, match="recognized angular momentum"):
+        basis.parse_basis_text("H 0\nQ 1 1.0\n 1.0 1.0\n****\n")
+    with pytest.raises(basis.BasisError, match="range of 1-100"):
+        basis.parse_basis_text("H 0\nS 0 1.0\n****\n")
+    with pytest.raises(basis.BasisError, match="positive exponents"):
+        basis.parse_basis_text("H 0\nS 1 1.0\n -1.0 1.0\n****\n")
+    with pytest.raises(basis.BasisError, match="could not be found"):
+        basis.read_basis("/nonexistent/basis")
+
+
+def test_builtin_bases_shell_structure():
+    b = basis.builtin_basis("6-31G*")
+    assert [(s.l, len(s.exps)) for s in b.elements[8]] == [(0, 6), (0, 3), (1, 3), (0, 1), (1, 1), (2, 1)]
+    assert [(s.l, len(s.exps)) for s in b.elements[1]] == [(0, 3), (0, 1)]
+    assert [(s.l, len(s.exps)) for s in basis.builtin_basis("STO-3G").elements[6]] == [(0, 3), (0, 3), (1, 3)]
+    with pytest.raises(basis.BasisError):
+        basis.builtin_basis("cc-pVQZ")
+
+
+def test_read_xyz(tmp_path):
+    p = tmp_path / "w.xyz"
+    p.write_text("3\n\nO 0 0 0\nH 0.7576 0.5870 0\nH -0.7576 0.5870 0\n")
+    m = basis.read_xyz(str(p))
+    assert m.Z == [8, 1, 1]
+    assert m.xyz[1][0] == pytest.approx(0.7576 * 1.889726126)
+    bad = tmp_path / "b.xyz"
+    bad.write_text("2\n\nO 0 0 0\n")
+    with pytest.raises(basis.GeometryError, match="atoms expected"):
+        basis.read_xyz(str(bad))
+    bad.write_text("1\n\nXx 0 0 0\n")
+    with pytest.raises(basis.GeometryError, match="not a valid element"):
+        basis.read_xyz(str(bad))
+
+
+def test_basis_function_counts():
+    w = geometry.water_cluster(3, 3, 2, 16, 0)
+    b = basis.builtin_basis("6-31G*")
+    assert shells.build_shells(w, b, pure=True).nbf() == 288
+    assert shells.build_shells(w, b, pure=False).nbf() == 304
+    assert shells.build_shells(w, b, pure=False).nshell == 160
+    w32 = geometry.water_cluster(4, 4, 2, 32, 0)
+    assert shells.build_shells(w32, b, pure=False).nbf() == 608
+    assert shells.build_shells(geometry.water(), basis.builtin_basis("STO-3G")).nbf() == 7
+
+
+def test_water_cluster_is_seeded_and_physical():
+    a = geometry.water_cluster(3, 3, 2, 16, 5)
+    b = geometry.water_cluster(3, 3, 2, 16, 5)
+    assert a.xyz == b.xyz
+    X = np.array(a.xyz) / basis.A_TO_BOHR
+    Z = np.array(a.Z)
+    d = np.linalg.norm(X[:, None] - X[None], axis=-1)
+    np.fill_diagonal(d, 99)
+    assert d.min() > 0.9  # no clashes
+    oh = d[np.ix_(Z == 8, Z == 1)].min(axis=0)
+    assert np.allclose(oh, 0.9572, atol=1e-3)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 10])
+def test_alkane_generator(n):
+    m = geometry.alkane(n, 0, jitter=0.0)
+    Z = np.array(m.Z)
+    assert (Z == 6).sum() == n and (Z == 1).sum() == 2 * n + 2
+    X = np.array(m.xyz) / basis.A_TO_BOHR
+    d = np.linalg.norm(X[:, None] - X[None], axis=-1)
+    ch = d[np.ix_(Z == 1, Z == 6)].min(axis=1)
+    assert np.allclose(ch, 1.09, atol=1e-6)
+    if n > 1:
+        cc = np.sort(d[np.ix_(Z == 6, Z == 6)], axis=1)[:, 1]
+        assert np.allclose(cc, 1.54, atol=1e-6)
+
+
+def test_displacements():
+    m = geometry.water_dimer(0)
+    ds = geometry.displacements(m, 0.005)
+    assert len(ds) == 36
+    delta = np.array(ds[0].xyz) - np.array(m.xyz)
+    assert delta[0, 0] == pytest.approx(0.005) and np.count_nonzero(delta) == 1
+
+
+def test_packed_layout_roundtrip():
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((7, 7))
+    A = A + A.T
+    p = shells.pack(A)
+    # element (y <= x) at x(x+1)/2 + y
+    assert p[shells.packed_index(2, 5)] == A[2, 5]
+    assert p[5 * 6 // 2 + 2] == A[2, 5]
+    assert np.array_equal(shells.unpack(p, 7), A)
