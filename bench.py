@@ -60,27 +60,20 @@ def _dist_env():
 
 # ---------------------------------------------------------------- reference arm
 def _ref_worker(args):
-    import numpy as np  # noqa: F401
-
-    rows, seconds_budget = args
+    seconds_budget, seed = args
     sys.path.insert(0, ROOT)
     from oracle import refpy
 
     _, sh = _workload()
     refpy.setup(sh, build_tensor=False)
-    done = 0
-    secs = 0.0
-    for (i0, i1) in rows:
-        n, s, _ = refpy.time_eri_rows(i0, i1)
-        done += n
-        secs += s
-        if secs > seconds_budget:
-            break
-    return done, secs
+    n, secs, _ = refpy.time_eri_random(seconds_budget, seed)
+    return n, secs
 
 
 def reference_rate(budget_s: float = 12.0, cores: int = 0):
-    """Reference ERI-phase throughput on the host: returns (builds/s, quartets/s, cores, sample)."""
+    """Reference ERI-phase throughput on the host cores, one process per core
+    (the reference's global state rules out threads).  Returns
+    (builds/s, quartets/s, cores, sample description)."""
     import multiprocessing as mp
 
     from oracle import refpy
@@ -92,19 +85,16 @@ def reference_rate(budget_s: float = 12.0, cores: int = 0):
     npair = n * (n + 1) // 2
     total_quartets = npair * (npair + 1) // 2
     cores = cores or os.cpu_count() or 1
-    # Rows i spread over the index range; each worker takes every cores-th row.
-    rows = [(i, i + 1) for i in range(n - 1, -1, -max(1, n // (4 * cores)))]
-    chunks = [[rows[j] for j in range(k, len(rows), cores)] for k in range(cores)]
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(c, budget_s) for c in chunks])
+        res = pool.map(_ref_worker, [(budget_s, 1000003 * (k + 1)) for k in range(cores)])
     done = sum(r[0] for r in res)
-    per_proc_rate = sum(r[0] / r[1] for r in res if r[1] > 0)  # quartets/s summed over processes
-    builds = per_proc_rate / total_quartets
-    sample = (f"{done} of {total_quartets} unique function quartets of the ERI phase "
-              f"(assignExactRepulsionTensor rows spread over i), {cores} processes x ~{budget_s:.0f}s; "
-              f"scaled to one full build, ERI phase only")
-    return builds, per_proc_rate, cores, sample
+    rate = sum(r[0] / r[1] for r in res if r[1] > 0)  # quartets/s over all processes
+    builds = rate / total_quartets
+    sample = (f"{done} uniformly drawn canonical function quartets (of {total_quartets}) of the reference's "
+              f"ERI phase (electronRepulsionIntegral), {cores} processes x {budget_s:.0f}s; scaled to one "
+              f"full Fock build, ERI phase only")
+    return builds, rate, cores, sample
 
 
 def run_reference(args):

@@ -23,6 +23,11 @@ class DssError(RuntimeError):
         self.code = code
 
 
+class DssScfOpts(ctypes.Structure):
+    _fields_ = [("conv", ctypes.c_double), ("diis_size", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("use_guess", ctypes.c_int)]
+
+
 class DssOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("schwarz_threshold", ctypes.c_double), ("boys_mode", ctypes.c_int)]
 
@@ -80,5 +85,12 @@ def load():
     L.dss_profile_build.restype = ctypes.c_int
     L.dss_probe_fp64_peak.argtypes = [vp, dp]
     L.dss_probe_fp64_peak.restype = ctypes.c_int
+    L.dss_one_electron.argtypes = [vp, ctypes.c_int, ip, dp, dp, dp, dp, dp]
+    L.dss_one_electron.restype = ctypes.c_int
+    L.dss_default_scf_opts.argtypes = [ctypes.POINTER(DssScfOpts)]
+    L.dss_default_scf_opts.restype = None
+    L.dss_scf_solve.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(DssScfOpts), dp, dp,
+                                ip]
+    L.dss_scf_solve.restype = ctypes.c_int
     _lib = L
     return L

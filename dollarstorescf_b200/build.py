@@ -109,7 +109,8 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     gen_stamp = os.path.join(GEN, "stamp")
     want = _stamp([os.path.join(CSRC, "gen_eri.py"), os.path.join(CSRC, "gen_boys_tab.py")], str(lmax))
     have = open(gen_stamp).read() if os.path.isfile(gen_stamp) else ""
-    if have != want or not (os.path.isfile(eri_gen) and os.path.isfile(boys_tab)):
+    sph_tab = os.path.join(GEN, "sph_tab.h")
+    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, sph_tab)):
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_eri.py"), eri_gen, str(lmax)])
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_boys_tab.py"), boys_tab])
         with open(gen_stamp, "w") as f:
@@ -127,7 +128,7 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
         if name.endswith(".cu"):
             units.append(os.path.join(CSRC, name))
     headers = [os.path.join(CSRC, n) for n in sorted(os.listdir(CSRC)) if n.endswith((".cuh", ".h"))]
-    headers += [eri_gen, boys_tab, os.path.join(INCLUDE, "dss.h")]
+    headers += [eri_gen, boys_tab, sph_tab, os.path.join(INCLUDE, "dss.h")]
     all_stamp = _stamp(headers, " ".join(CFLAGS + ARCH))
     # The generated class units only see the kernel headers.
     kernel_headers = [os.path.join(CSRC, n) for n in ("eri_kernels.cuh", "common.cuh", "boys.cuh")]
@@ -153,7 +154,7 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     jobs = jobs or max(1, os.cpu_count() or 1)
     with ThreadPoolExecutor(jobs) as ex:
         objs = list(ex.map(compile_one, units))
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread"]
     subprocess.check_call(cmd)
     return LIB
 

@@ -47,7 +47,21 @@ __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __rest
   if (packed && r <= c) packed[(long long)c * (c + 1) / 2 + r] = v;
 }
 
+__global__ void combine_g_kernel(const double* __restrict__ J, const double* __restrict__ K, double* __restrict__ G,
+                                 int n) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * n) return;
+  const int r = (int)(idx / n), c = (int)(idx % n);
+  const long long t = (long long)c * n + r;
+  G[idx] = (J[idx] + J[t]) - 0.5 * (K[idx] + K[t]);
+}
+
 }  // namespace
+
+void dss_symmetrize_combine(cudaStream_t s, int n, const double* Jacc, const double* Kacc, double* G) {
+  const long long nn = (long long)n * n;
+  combine_g_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(Jacc, Kacc, G, n);
+}
 
 // ------------------------------------------------------------------ helpers
 int dss_fail(dss_ctx* ctx, int code, const std::string& msg) {
@@ -122,6 +136,11 @@ int dss_create(dss_ctx** out, const dss_opts* opts) {
   }
   e = cudaSetDevice(ctx->opts.device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  for (int i = 0; i < dss_ctx::kSideStreams && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
   ctx->stream = ctx->own_stream;
   if (e != cudaSuccess) {
     g_create_error = std::string("dss_create: ") + cudaGetErrorString(e);
@@ -137,6 +156,11 @@ void dss_destroy(dss_ctx* ctx) {
   cudaSetDevice(ctx->opts.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->release();
+  for (int i = 0; i < dss_ctx::kSideStreams; ++i) {
+    if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+    if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
+  }
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -192,6 +216,7 @@ int dss_set_basis(dss_ctx* ctx, int n_shell, const int* l, const int* nprim, con
     f0 += pure ? 2 * l[s] + 1 : (l[s] + 1) * (l[s] + 2) / 2;
   }
   B.nbf = f0;
+  ctx->basis = B;
   int rc = dss_setup_pairs(ctx, std::move(B));
   if (rc != DSS_OK) return rc;
   return DSS_OK;
@@ -463,9 +488,26 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   const size_t nn = (size_t)n * n;
   DSS_CUDA(cudaMemsetAsync(Jacc, 0, nn * sizeof(double), ctx->stream));
   DSS_CUDA(cudaMemsetAsync(Kacc, 0, nn * sizeof(double), ctx->stream));
-  for (size_t ci = 0; ci < ctx->tasks.size(); ++ci) {
+  // Launch order: highest total angular momentum first (longest per-quartet
+  // latency), spread round-robin over the side streams; profiling (events)
+  // keeps every launch on the main stream so each is timed alone.
+  std::vector<int> order;
+  for (size_t ci = 0; ci < ctx->tasks.size(); ++ci)
+    if (ctx->tasks[ci].ntasks) order.push_back((int)ci);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const ClassTasks& a = ctx->tasks[x];
+    const ClassTasks& b = ctx->tasks[y];
+    return a.la + a.lb + a.lc + a.ld > b.la + b.lb + b.lc + b.ld;
+  });
+  const bool fork = events == nullptr;
+  if (fork) {
+    DSS_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    for (int i = 0; i < dss_ctx::kSideStreams; ++i) DSS_CUDA(cudaStreamWaitEvent(ctx->side[i], ctx->fork_ev, 0));
+  }
+  int slot = 0;
+  for (int ci : order) {
     ClassTasks& ct = ctx->tasks[ci];
-    if (!ct.ntasks) continue;
+    cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
     EriArgs a;
     a.tasks = ct.d_tasks.ptr;
     a.ntasks = ct.ntasks;
@@ -480,10 +522,16 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.J = Jacc;
     a.K = Kacc;
     a.n = n;
-    if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], ctx->stream));
-    dss_launch_eri_jk(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, a, ctx->stream);
+    if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], st));
+    dss_launch_eri_jk(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, a, st);
     DSS_CUDA(cudaGetLastError());
-    if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], ctx->stream));
+    if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], st));
+  }
+  if (fork) {
+    for (int i = 0; i < dss_ctx::kSideStreams; ++i) {
+      DSS_CUDA(cudaEventRecord(ctx->join_ev[i], ctx->side[i]));
+      DSS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join_ev[i], 0));
+    }
   }
   return DSS_OK;
 }

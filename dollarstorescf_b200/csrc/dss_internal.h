@@ -66,14 +66,26 @@ struct ClassTasks {
   DevBuf<int4> d_tasks;
 };
 
+struct ScfBuffers {
+  DevBuf<double> pool;
+  DevBuf<int> ibuf;
+};
+
 struct dss_ctx {
   dss_opts opts{};
   cudaStream_t stream = nullptr;      // the stream work is enqueued on
   cudaStream_t own_stream = nullptr;  // created with the context
+  // Side streams: the class launches of one build fork onto them so that the
+  // long-running, low-occupancy high-angular-momentum classes overlap the rest.
+  static constexpr int kSideStreams = 6;
+  cudaStream_t side[kSideStreams] = {};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[kSideStreams] = {};
   std::string err;
 
   // basis
   int nbf = 0, pure = 1, nshell = 0;
+  BasisHost basis;
   DevBuf<PrimPair> d_pp;
   DevBuf<int> d_pair_a, d_pair_b, d_pair_pp0, d_pair_npp, d_sh_f0;
   DevBuf<double> d_sh_xyz, d_Q;
@@ -85,6 +97,7 @@ struct dss_ctx {
 
   // build scratch
   DevBuf<double> packed_in, packed_j, packed_k, Ddense, Jacc, Kacc;
+  ScfBuffers scf;
 
   void release_basis() {
     d_pp.free();
@@ -106,6 +119,8 @@ struct dss_ctx {
     Ddense.free();
     Jacc.free();
     Kacc.free();
+    scf.pool.free();
+    scf.ibuf.free();
   }
 };
 
@@ -113,6 +128,8 @@ int dss_fail(dss_ctx* ctx, int code, const std::string& msg);
 int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what);
 int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
 int dss_build_tasks(dss_ctx* ctx);
+// G = (Jacc + Jacc^T) - (Kacc + Kacc^T) / 2, dense n x n.
+void dss_symmetrize_combine(cudaStream_t s, int n, const double* Jacc, const double* Kacc, double* G);
 // Enqueues one J/K accumulation; with events != NULL records events[2i], events[2i+1]
 // around the launch of class i.
 int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events = nullptr);

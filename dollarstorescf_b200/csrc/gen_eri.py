@@ -29,6 +29,7 @@ Usage: python gen_eri.py OUT.cuh [LMAX]
 from __future__ import annotations
 
 import math
+import os
 import sys
 from typing import Dict, List, Tuple
 
@@ -372,6 +373,24 @@ def main() -> None:
     lines.append("")
     with open(out_path, "w") as f:
         f.write("\n".join(lines) + "\n")
+    write_sph_table(os.path.join(os.path.dirname(os.path.abspath(out_path)), "sph_tab.h"), lmax)
+
+
+def write_sph_table(path: str, lmax: int) -> None:
+    """Host table of the function transforms: for each l <= lmax and each output
+    function (5D: m = -l..l; 6D: monomials), the (Cartesian index, weight) terms."""
+    out = ["// Generated by gen_eri.py -- do not edit.", "#pragma once", "",
+           "struct DssSphTerm { int l; int func; int cart; double w; int pure; };",
+           "static const DssSphTerm kDssSphTerms[] = {"]
+    for pure in (1, 0):
+        for l in range(lmax + 1):
+            for fidx, row in enumerate(transform_rows(l, bool(pure))):
+                for ci, w in row:
+                    out.append(f"  {{{l}, {fidx}, {ci}, {lit(w)}, {pure}}},")
+    out.append("};")
+    out.append("static const int kDssSphTermCount = sizeof(kDssSphTerms) / sizeof(kDssSphTerms[0]);")
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,384 @@
+// Device RHF SCF: the reference's solveMOs loop (chem/scf/SCFSolver.cpp:196-237)
+// with every matrix step on the GPU.
+//
+// Per iteration (runSCFIteration, SCFSolver.cpp:145-172):
+//   G = J[2 D] - K[2 D] / 2                 (computeCoulombTerms/ExchangeTerms :29-43)
+//   F_new = H + G                            (updateFockMatrix :45-62)
+//   iteration 1: F = F_new; later: Pulay DIIS (SCFDIIS.cpp:19-52, lalib/DIIS.ipp):
+//     e = S D F_new - (S D F_new)^T, B_ii = |e|^2, B_ij = <e_i, e_j>, bordered by
+//     ones; ring of diis_size entries, when full the entry with the largest B_ii
+//     is replaced; F = sum_i c_i F_i from B c = (0,..,0,1).
+//   F' = X F X, X = S^-1/2 (Loewdin, SCFBasis.cpp:85-100); F' C' = C' eps
+//   (cyclic Jacobi on the device, warm-started from the previous C'); C = X C'
+//   D = C_occ C_occ^T                        (computeDensityMatrix :77-94)
+//   E_elec = 2 sum_occ eps - tr(D G)         (getTotalElectronicEnergy :118-130)
+//   converged when |E_elec - E_prev| < conv  (checkConvergence :174-177)
+// Final energy from the final density (calculateEnergies, Energy.cpp:21-50):
+//   E = 2 tr(D H) + tr(D G[D]) + E_nuc.
+// Unlike the reference the loop has an iteration cap (DSS_ERR_NOCONV), and a
+// singular DIIS system falls back to the newest Fock matrix instead of the
+// reference's behaviour (LAPACK reports the error, the coefficients stay the
+// right-hand side and F becomes 0, lalib/Lapack.cpp:164-169).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "dss.h"
+#include "dss_internal.h"
+#include "linalg.cuh"
+
+namespace {
+
+__global__ void unpack_sym(const double* __restrict__ p, double* __restrict__ d, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  const int x = r > c ? r : c, y = r > c ? c : r;
+  d[t] = p[(long long)x * (x + 1) / 2 + y];
+}
+
+__global__ void pack_sym(const double* __restrict__ d, double* __restrict__ p, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  if (r <= c) p[(long long)c * (c + 1) / 2 + r] = d[t];
+}
+
+// out = a*X + b*Y (+ c*Z if Z)
+__global__ void axpby(long long N, double a, const double* X, double b, const double* Y, double c, const double* Z,
+                      double* out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  double v = a * X[t] + b * Y[t];
+  if (Z) v += c * Z[t];
+  out[t] = v;
+}
+
+// e = T - T^T
+__global__ void antisym(const double* __restrict__ T, double* __restrict__ e, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  e[t] = T[t] - T[(long long)c * n + r];
+}
+
+// X = U diag(s^-1/2) U^T helper: scale columns of U by f(s).
+__global__ void scale_cols(const double* __restrict__ U, const double* __restrict__ s, double* __restrict__ out,
+                           int n, int power_neg_half) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int c = (int)(t % n);
+  const double v = power_neg_half ? 1.0 / sqrt(s[c]) : sqrt(s[c]);
+  out[t] = U[t] * v;
+}
+
+// D = C[:, :nocc] C[:, :nocc]^T
+__global__ void density_kernel(const double* __restrict__ C, double* __restrict__ D, int n, int nocc) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  double v = 0.0;
+  for (int k = 0; k < nocc; ++k) v += C[(size_t)r * n + k] * C[(size_t)c * n + k];
+  D[t] = v;
+}
+
+// Block sums of x*y (and optional second pair) into out[] via atomics.
+__global__ void dot_kernel(long long N, const double* __restrict__ x, const double* __restrict__ y, double* out) {
+  double acc = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+    acc += x[t] * y[t];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+    atomicAdd(out, s);
+  }
+}
+
+// DIIS slot choice (lalib/DIIS.ipp:19-62): state[0] = count, state[1] = slot.
+__global__ void diis_choose(int* state, const double* B, int size, int ld) {
+  int count = state[0];
+  int slot = 0;
+  if (count < size) {
+    slot = count;
+    count += 1;
+  } else {
+    double mx = 0.0;
+    for (int i = 0; i < size; ++i) {
+      const double e = B[i * ld + i];
+      if (e > mx) {
+        mx = e;
+        slot = i;
+      }
+    }
+  }
+  state[0] = count;
+  state[1] = slot;
+}
+
+// B row/column of the new slot from the dot products, then the bordered solve
+// B c = (0,..,0,1) by Gaussian elimination with partial pivoting.
+__global__ void diis_solve(int* state, double* B, int ld, const double* dots, double* coef) {
+  const int count = state[0], slot = state[1];
+  for (int i = 0; i < count; ++i) {
+    B[slot * ld + i] = dots[i];
+    B[i * ld + slot] = dots[i];
+  }
+  const int m = count + 1;
+  double M[10][11];
+  for (int i = 0; i < m; ++i) {
+    for (int j = 0; j < m; ++j) {
+      double v;
+      if (i < count && j < count) v = B[i * ld + j];
+      else if (i == count && j == count) v = 0.0;
+      else v = 1.0;
+      M[i][j] = v;
+    }
+    M[i][m] = (i == count) ? 1.0 : 0.0;
+  }
+  bool singular = false;
+  for (int k = 0; k < m && !singular; ++k) {
+    int piv = k;
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(M[i][k]) > fabs(M[piv][k])) piv = i;
+    if (M[piv][k] == 0.0) {
+      singular = true;
+      break;
+    }
+    if (piv != k)
+      for (int j = 0; j <= m; ++j) {
+        const double t = M[k][j];
+        M[k][j] = M[piv][j];
+        M[piv][j] = t;
+      }
+    for (int i = k + 1; i < m; ++i) {
+      const double f = M[i][k] / M[k][k];
+      for (int j = k; j <= m; ++j) M[i][j] -= f * M[k][j];
+    }
+  }
+  if (!singular) {
+    for (int i = m - 1; i >= 0; --i) {
+      double v = M[i][m];
+      for (int j = i + 1; j < m; ++j) v -= M[i][j] * coef[j];
+      coef[i] = v / M[i][i];
+    }
+  }
+  for (int i = 0; i < count; ++i) {
+    if (singular) coef[i] = (i == slot) ? 1.0 : 0.0;
+  }
+  state[2] = singular ? 1 : 0;
+}
+
+// F = sum_i coef[i] F_i
+__global__ void diis_combine(int n2, const double* __restrict__ Fring, const double* __restrict__ coef,
+                             const int* __restrict__ state, double* __restrict__ F) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n2) return;
+  const int count = state[0];
+  double v = 0.0;
+  for (int i = 0; i < count; ++i) v += coef[i] * Fring[(size_t)i * n2 + t];
+  F[t] = v;
+}
+
+__global__ void copy_slot(int n2, const double* __restrict__ src, double* __restrict__ ring, const int* state) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n2) return;
+  ring[(size_t)state[1] * n2 + t] = src[t];
+}
+
+// dots[i] = <e_i, e_new> for the ring entries (i < count), after the new entry is stored.
+__global__ void ring_dots(int n2, const double* __restrict__ ering, const int* __restrict__ state,
+                          double* __restrict__ dots) {
+  const int i = blockIdx.y;
+  if (i >= state[0]) return;
+  const double* a = ering + (size_t)i * n2;
+  const double* b = ering + (size_t)state[1] * n2;
+  double acc = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+    acc += a[t] * b[t];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+    atomicAdd(dots + i, s);
+  }
+}
+
+// E_elec = 2 sum_{i<nocc} eps_i - tr(D G)  ->  out[0]; tr(D G) comes in trDG.
+__global__ void energy_kernel(const double* eps, int nocc, const double* trDG, double* out) {
+  double s = 0.0;
+  for (int i = 0; i < nocc; ++i) s += 2.0 * eps[i];
+  out[0] = s - trDG[0];
+}
+
+inline unsigned nb(long long N, int t = 256) { return (unsigned)((N + t - 1) / t); }
+
+}  // namespace
+
+extern "C" {
+
+void dss_default_scf_opts(dss_scf_opts* o) {
+  if (!o) return;
+  o->conv = 1e-8;  // scf::energy_threshold, chem/scf/SCFSolver.cpp:26
+  o->diis_size = 8;  // diis::setIterationCount(8), SCFSolver.cpp:214
+  o->max_iter = 128;
+  o->use_guess = 0;
+}
+
+int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha, double e_nuc,
+                  const dss_scf_opts* opts_in, double* E_total, double* Dp, int* iterations) {
+  if (!ctx) return DSS_ERR_INVALID;
+  ctx->err.clear();
+  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_scf_solve: no basis set");
+  if (!Hp || !Sp || !E_total) return dss_fail(ctx, DSS_ERR_INVALID, "dss_scf_solve: NULL argument");
+  const int n = ctx->nbf;
+  if (n_alpha < 0 || n_alpha > n) return dss_fail(ctx, DSS_ERR_INVALID, "dss_scf_solve: occupied count out of range");
+  dss_scf_opts o;
+  dss_default_scf_opts(&o);
+  if (opts_in) o = *opts_in;
+  if (o.diis_size < 1 || o.diis_size > 9)
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_scf_solve: diis_size must be 1..9");
+  if (o.use_guess && !Dp) return dss_fail(ctx, DSS_ERR_INVALID, "dss_scf_solve: use_guess needs D");
+  if (cudaSetDevice(ctx->opts.device) != cudaSuccess) return dss_fail(ctx, DSS_ERR_CUDA, "dss_scf_solve: cudaSetDevice");
+  const size_t n2 = (size_t)n * n, np = (size_t)n * (n + 1) / 2;
+  cudaStream_t s = ctx->stream;
+  // Device buffers (kept in the context so repeated solves reuse them).
+  ScfBuffers& b = ctx->scf;
+  const int ds = o.diis_size;
+  const size_t need = n2 * (14 + 2 * (size_t)ds) + 3 * n2 + 8 * (size_t)n + 256;
+  if (b.pool.resize(need) != cudaSuccess || b.ibuf.resize(8 + 2 * (size_t)n) != cudaSuccess)
+    return dss_fail(ctx, DSS_ERR_OOM, "dss_scf_solve: device allocation failed");
+  double* base = b.pool.ptr;
+  double *H = base, *S = H + n2, *X = S + n2, *D = X + n2, *Dt = D + n2, *J = Dt + n2, *K = J + n2, *G = K + n2,
+         *F = G + n2, *Fn = F + n2, *T1 = Fn + n2, *T2 = T1 + n2, *Cp = T2 + n2, *C = Cp + n2;
+  double* Fring = C + n2;
+  double* Ering = Fring + (size_t)ds * n2;
+  double* work = Ering + (size_t)ds * n2;           // 3 n^2 + 64 + n ints
+  double* eps = work + 3 * n2 + 64 + (size_t)n;    // n
+  double* small = eps + n;                           // scalars: [0]=E, [1]=trDG, [2..11] dots, [16..35] coef
+  double* Bm = small + 64;                           // 10 x 10
+  int* state = b.ibuf.ptr;
+  auto fail_cuda = [&](cudaError_t e, const char* what) {
+    return dss_fail(ctx, DSS_ERR_CUDA, std::string("dss_scf_solve: ") + what + ": " + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+#define SCF_CHECK(call, what)                      \
+  do {                                             \
+    e = (call);                                    \
+    if (e != cudaSuccess) return fail_cuda(e, what); \
+  } while (0)
+  // Inputs.
+  DevBuf<double> packed;
+  SCF_CHECK(packed.resize(np), "alloc");
+  SCF_CHECK(cudaMemcpyAsync(packed.ptr, Hp, np * 8, cudaMemcpyHostToDevice, s), "H2D H");
+  unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, H, n);
+  SCF_CHECK(cudaMemcpyAsync(packed.ptr, Sp, np * 8, cudaMemcpyHostToDevice, s), "H2D S");
+  unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, S, n);
+  // X = U s^-1/2 U^T from the eigen-decomposition of S (assignOrthogonalization).
+  SCF_CHECK(cudaMemcpyAsync(T1, S, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy S");
+  SCF_CHECK(dss_jacobi_eigh(s, n, T1, T2, eps, work, 60, 1e-15, false), "eigh(S)");
+  scale_cols<<<nb(n2), 256, 0, s>>>(T2, eps, T1, n, 1);
+  dss_gemm(s, n, false, true, 1.0, T1, T2, 0.0, X);
+  // Initial density.
+  if (o.use_guess) {
+    SCF_CHECK(cudaMemcpyAsync(packed.ptr, Dp, np * 8, cudaMemcpyHostToDevice, s), "H2D D");
+    unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, D, n);
+  } else {
+    SCF_CHECK(cudaMemsetAsync(D, 0, n2 * 8, s), "zero D");  // useCoreGuess, SCFSolver.cpp:179-194
+  }
+  SCF_CHECK(cudaMemsetAsync(state, 0, 8 * sizeof(int), s), "zero state");
+  SCF_CHECK(cudaMemsetAsync(Bm, 0, 100 * 8, s), "zero B");
+  bool have_cp = false;
+  double E = 0.0, E_prev = 0.0;
+  int it = 0;
+  int rc = DSS_OK;
+  while (true) {
+    if (it && std::fabs(E - E_prev) < o.conv) break;
+    if (it >= o.max_iter) {
+      rc = dss_fail(ctx, DSS_ERR_NOCONV, "dss_scf_solve: no convergence within max_iter iterations");
+      break;
+    }
+    ++it;
+    // G = J[2D] - K[2D]/2
+    axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 2.0, D, 0.0, D, 0.0, nullptr, Dt);
+    int r2 = dss_enqueue_jk(ctx, Dt, J, K);
+    if (r2 != DSS_OK) return r2;
+    // J, K hold the accumulators: G = (J + J^T) - (K + K^T)/2
+    dss_symmetrize_combine(s, n, J, K, G);
+    axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 1.0, H, 1.0, G, 0.0, nullptr, Fn);
+    if (it == 1) {
+      SCF_CHECK(cudaMemcpyAsync(F, Fn, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy F");
+    } else {
+      // e = S D F_new - (S D F_new)^T
+      dss_gemm(s, n, false, false, 1.0, D, Fn, 0.0, T1);
+      dss_gemm(s, n, false, false, 1.0, S, T1, 0.0, T2);
+      diis_choose<<<1, 1, 0, s>>>(state, Bm, ds, 10);
+      antisym<<<nb(n2), 256, 0, s>>>(T2, T1, n);
+      copy_slot<<<nb(n2), 256, 0, s>>>((int)n2, T1, Ering, state);
+      copy_slot<<<nb(n2), 256, 0, s>>>((int)n2, Fn, Fring, state);
+      SCF_CHECK(cudaMemsetAsync(small + 2, 0, 10 * 8, s), "zero dots");
+      ring_dots<<<dim3(64, ds), 256, 0, s>>>((int)n2, Ering, state, small + 2);
+      diis_solve<<<1, 1, 0, s>>>(state, Bm, 10, small + 2, small + 16);
+      diis_combine<<<nb(n2), 256, 0, s>>>((int)n2, Fring, small + 16, state, F);
+    }
+    // F' = X F X, eigen-decomposition (warm start from the previous C').
+    dss_gemm(s, n, false, false, 1.0, F, X, 0.0, T1);
+    dss_gemm(s, n, false, false, 1.0, X, T1, 0.0, T2);  // T2 = F'
+    if (have_cp) {
+      dss_gemm(s, n, false, false, 1.0, T2, Cp, 0.0, T1);
+      dss_gemm(s, n, true, false, 1.0, Cp, T1, 0.0, T2);  // Cp^T F' Cp
+      SCF_CHECK(dss_jacobi_eigh(s, n, T2, T1, eps, work, 40, 1e-15, false), "eigh(F')");
+      dss_gemm(s, n, false, false, 1.0, Cp, T1, 0.0, T2);
+      SCF_CHECK(cudaMemcpyAsync(Cp, T2, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy C'");
+    } else {
+      SCF_CHECK(dss_jacobi_eigh(s, n, T2, Cp, eps, work, 60, 1e-15, false), "eigh(F')");
+      have_cp = true;
+    }
+    dss_gemm(s, n, false, false, 1.0, X, Cp, 0.0, C);
+    density_kernel<<<nb(n2), 256, 0, s>>>(C, D, n, n_alpha);
+    // E_elec = 2 sum eps_occ - tr(D G), G from the previous density.
+    SCF_CHECK(cudaMemsetAsync(small + 1, 0, 8, s), "zero tr");
+    dot_kernel<<<64, 256, 0, s>>>((long long)n2, D, G, small + 1);
+    energy_kernel<<<1, 1, 0, s>>>(eps, n_alpha, small + 1, small);
+    SCF_CHECK(cudaGetLastError(), "launch");
+    double Eh = 0.0;
+    SCF_CHECK(cudaMemcpyAsync(&Eh, small, 8, cudaMemcpyDeviceToHost, s), "D2H E");
+    SCF_CHECK(cudaStreamSynchronize(s), "sync");
+    E_prev = E;
+    E = Eh;
+    if (!std::isfinite(E)) {
+      rc = dss_fail(ctx, DSS_ERR_NOCONV, "dss_scf_solve: energy is not finite");
+      break;
+    }
+  }
+  // Final energy from the final density (calculateEnergies).
+  axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 2.0, D, 0.0, D, 0.0, nullptr, Dt);
+  int r3 = dss_enqueue_jk(ctx, Dt, J, K);
+  if (r3 != DSS_OK) return r3;
+  dss_symmetrize_combine(s, n, J, K, G);
+  SCF_CHECK(cudaMemsetAsync(small + 1, 0, 16, s), "zero tr");
+  dot_kernel<<<64, 256, 0, s>>>((long long)n2, D, H, small + 1);
+  dot_kernel<<<64, 256, 0, s>>>((long long)n2, D, G, small + 2);
+  double tr[2];
+  SCF_CHECK(cudaMemcpyAsync(tr, small + 1, 16, cudaMemcpyDeviceToHost, s), "D2H tr");
+  if (Dp) {
+    pack_sym<<<nb(n2), 256, 0, s>>>(D, packed.ptr, n);
+    SCF_CHECK(cudaMemcpyAsync(Dp, packed.ptr, np * 8, cudaMemcpyDeviceToHost, s), "D2H D");
+  }
+  SCF_CHECK(cudaStreamSynchronize(s), "sync");
+  *E_total = 2.0 * tr[0] + tr[1] + e_nuc;
+  if (iterations) *iterations = it;
+#undef SCF_CHECK
+  return rc;
+}
+
+}  // extern "C"

@@ -127,6 +127,35 @@ class FockBuilder:
         self._check(self._L.dss_probe_fp64_peak(self._h, ctypes.byref(t)))
         return t.value
 
+    def one_electron(self, sh: ShellArrays):
+        """(S, T, V, E_nuc) packed-U for the molecule of ``sh`` (the current basis)."""
+        n = self.nbf
+        np_ = n * (n + 1) // 2
+        S, T, V = np.empty(np_), np.empty(np_), np.empty(np_)
+        en = ctypes.c_double()
+        Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
+        xyz = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
+        self._check(self._L.dss_one_electron(self._h, sh.natom, _ip(Z), _dp(xyz), _dp(S), _dp(T), _dp(V),
+                                             ctypes.byref(en)))
+        return S, T, V, en.value
+
+    def scf(self, H: np.ndarray, S: np.ndarray, n_alpha: int, e_nuc: float, conv: float = 1e-8,
+            diis_size: int = 8, max_iter: int = 128, guess: Optional[np.ndarray] = None,
+            raise_on_noconv: bool = True):
+        """Device RHF.  Returns (E_total, D_alpha packed-U, iterations, status)."""
+        n = self.nbf
+        o = _lib.DssScfOpts(conv, diis_size, max_iter, 1 if guess is not None else 0)
+        D = np.ascontiguousarray(guess, dtype=np.float64).copy() if guess is not None else np.zeros(n * (n + 1) // 2)
+        E = ctypes.c_double()
+        it = ctypes.c_int()
+        Hc = np.ascontiguousarray(H, dtype=np.float64)
+        Sc = np.ascontiguousarray(S, dtype=np.float64)
+        rc = self._L.dss_scf_solve(self._h, _dp(Hc), _dp(Sc), int(n_alpha), float(e_nuc), ctypes.byref(o),
+                                   ctypes.byref(E), _dp(D), ctypes.byref(it))
+        if rc != 0 and (raise_on_noconv or rc != -4):
+            self._check(rc)
+        return E.value, D, it.value, rc
+
     def sync(self) -> None:
         self._check(self._L.dss_sync(self._h))
 

@@ -114,6 +114,38 @@ int dss_profile_build(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_d
  * loop (the FP64 CUDA-core roofline the ERI kernels are reported against). */
 int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops);
 
+/* One-electron matrices of the current basis for the given nuclei (Z[natom],
+ * xyz_bohr[3*natom]), packed-U: overlap S, kinetic T and nuclear attraction V
+ * (H = T + V), and the nuclear repulsion energy.  Replaces
+ * scf::assignOverlapMatrix / assignCoreHamiltonian (chem/scf/SCFBasis.cpp:56-83).
+ * Any output may be NULL.  Host computation, threaded over shell pairs. */
+int dss_one_electron(dss_ctx* ctx, int natom, const int* Z, const double* xyz_bohr, double* S_packed,
+                     double* T_packed, double* V_packed, double* e_nuc);
+
+/* ---------------------------------------------------------------- SCF on the device */
+
+typedef struct dss_scf_opts {
+  double conv;   /* converged when |E_elec - E_prev| < conv (scf::energy_threshold) */
+  int diis_size; /* Pulay DIIS ring length, 1..9 */
+  int max_iter;  /* iteration cap (the reference loops until converged) */
+  int use_guess; /* 0: core guess D = 0 (scf::useCoreGuess); 1: start from D_alpha_inout */
+} dss_scf_opts;
+
+/* Defaults: conv 1e-8 (chem/scf/SCFSolver.cpp:26), diis_size 8 (:214),
+ * max_iter 128, core guess. */
+void dss_default_scf_opts(dss_scf_opts* opts);
+
+/* Closed-shell RHF on the device for the current basis, replacing
+ * scf::useCoreGuess + scf::solveMOs + scf::getTotalEnergy
+ * (chem/scf/SCFSolver.cpp:179-237, chem/scf/Energy.cpp:21-78).
+ * H (core Hamiltonian) and S (overlap) packed-U; n_alpha occupied orbitals;
+ * e_nuc the nuclear repulsion added to the final energy.  On return
+ * *E_total holds the converged total energy, D_alpha_inout (if not NULL) the
+ * final alpha density (packed-U), *iterations the SCF iterations.
+ * Returns DSS_ERR_NOCONV when max_iter is reached (outputs still written). */
+int dss_scf_solve(dss_ctx* ctx, const double* H_packed, const double* S_packed, int n_alpha, double e_nuc,
+                  const dss_scf_opts* opts, double* E_total, double* D_alpha_inout, int* iterations);
+
 #ifdef __cplusplus
 }
 #endif

@@ -286,6 +286,47 @@ long long ref_time_eri_rows(int i_begin, int i_end, double* seconds, double* che
   return count;
 }
 
+// Timed random sample of the ERI phase: canonical quartets (ij|kl) with pair
+// indices m = i(i+1)/2 + j <= n = k(k+1)/2 + l drawn uniformly (xorshift64 from
+// seed) until max_seconds have passed.  The mean cost per quartet times the
+// quartet count gives the reference's ERI-phase time for the whole tensor.
+long long ref_time_eri_random(double max_seconds, unsigned long long seed, double* seconds, double* checksum) {
+  const size_t n = scf::basis.size();
+  const unsigned long long P = (unsigned long long)n * (n + 1) / 2;
+  unsigned long long st = seed ? seed : 88172645463325252ull;
+  auto next = [&]() {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    return st;
+  };
+  auto decode = [](unsigned long long m, uint& i, uint& j) {
+    i = (uint)((std::sqrt(8.0 * (double)m + 1.0) - 1.0) / 2.0);
+    while ((unsigned long long)i * (i + 1) / 2 > m) --i;
+    while ((unsigned long long)(i + 1) * (i + 2) / 2 <= m) ++i;
+    j = (uint)(m - (unsigned long long)i * (i + 1) / 2);
+  };
+  long long count = 0;
+  double sum = 0.0;
+  auto t0 = std::chrono::steady_clock::now();
+  double el = 0.0;
+  while (el < max_seconds) {
+    for (int rep = 0; rep < 64; ++rep) {
+      unsigned long long a = next() % P, b = next() % P;
+      if (a > b) std::swap(a, b);
+      uint i, j, k, l;
+      decode(a, i, j);
+      decode(b, k, l);
+      sum += flo::electronRepulsionIntegral(scf::basis[i], scf::basis[k], scf::basis[j], scf::basis[l]);
+      ++count;
+    }
+    el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  *seconds = el;
+  *checksum = sum;
+  return count;
+}
+
 // Timed J+K digest over the stored tensor for one density (the per-iteration
 // Fock work of the reference, SCFSolver.cpp:29-43).  Returns seconds.
 double ref_time_jk(const double* D_alpha_packed) {

@@ -51,6 +51,8 @@ def lib():
         L.ref_boys.restype = ctypes.c_double
         L.ref_time_eri_rows.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp]
         L.ref_time_eri_rows.restype = ctypes.c_longlong
+        L.ref_time_eri_random.argtypes = [ctypes.c_double, ctypes.c_ulonglong, dp, dp]
+        L.ref_time_eri_random.restype = ctypes.c_longlong
         L.ref_time_jk.argtypes = [dp]
         L.ref_time_jk.restype = ctypes.c_double
         _lib = L
@@ -151,4 +153,11 @@ def time_eri_rows(i_begin: int, i_end: int) -> Tuple[int, float, float]:
     s = ctypes.c_double()
     c = ctypes.c_double()
     n = lib().ref_time_eri_rows(i_begin, i_end, ctypes.byref(s), ctypes.byref(c))
+    return int(n), s.value, c.value
+
+
+def time_eri_random(max_seconds: float, seed: int) -> Tuple[int, float, float]:
+    s = ctypes.c_double()
+    c = ctypes.c_double()
+    n = lib().ref_time_eri_random(max_seconds, seed, ctypes.byref(s), ctypes.byref(c))
     return int(n), s.value, c.value
