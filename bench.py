@@ -144,7 +144,7 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.device),
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -245,6 +245,11 @@ def run_gpu(args):
     def one_build():
         fb.jk_device(Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
 
+    # Per-class kernel choice (untimed): thread-per-quartet vs warp-cooperative.
+    from dollarstorescf_b200 import autotune
+
+    variants = autotune.tune(fb, Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
+
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             flush.fill_(1.0)
@@ -320,6 +325,7 @@ def run_gpu(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded (H2O)16 cluster, 3x3x2 lattice 3.0 A, rotation + 0.2 A jitter)",
         "config": {"workload": WORKLOAD, "nbf": n, "shells": sh.nshell, "boys": "reference series",
+                   "warp_cooperative_classes": sorted(k for k, v in variants.items() if v == 1),
                    "l2": "flushed between steps (512 MiB write)", "parallelism": f"replicas x{ws}"},
         "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": npk * 8,
                 "d2h_bytes_per_step": 2 * npk * 8},
@@ -349,7 +355,7 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dss", choices=["dss", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -85,6 +85,10 @@ def load():
     L.dss_profile_build.restype = ctypes.c_int
     L.dss_probe_fp64_peak.argtypes = [vp, dp]
     L.dss_probe_fp64_peak.restype = ctypes.c_int
+    L.dss_set_class_variant.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.dss_set_class_variant.restype = ctypes.c_int
+    L.dss_get_class_variant.argtypes = [vp, ctypes.c_int]
+    L.dss_get_class_variant.restype = ctypes.c_int
     L.dss_one_electron.argtypes = [vp, ctypes.c_int, ip, dp, dp, dp, dp, dp]
     L.dss_one_electron.restype = ctypes.c_int
     L.dss_default_scf_opts.argtypes = [ctypes.POINTER(DssScfOpts)]

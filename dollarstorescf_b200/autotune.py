@@ -1,0 +1,63 @@
+"""Per-class kernel autotuner.
+
+For every shell-quartet class with work in the current basis, times each kernel
+variant the library offers (0: one thread per quartet, 1: one warp per quartet
+with shared-memory programs) with per-launch CUDA events (dss_profile_build runs
+the classes one after another on one stream) and keeps the faster one.  The
+choice depends on the class and on the quartet count, so it is redone per basis
+and can be cached by (class, pure, boys mode, quartet-count bucket).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from typing import Dict, Optional
+
+from .engine import FockBuilder
+
+
+def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
+         cache_path: Optional[str] = None, key_extra: str = "") -> Dict[str, int]:
+    """Chooses a variant per class; returns {class name: variant}."""
+    cache = {}
+    if cache_path and os.path.isfile(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    nc = fb.num_classes()
+    infos = [fb.class_info(i) for i in range(nc)]
+    names = ["%d%d%d%d" % tuple(info[0]) for info in infos]
+    keys = [f"{names[i]}|{key_extra}|q{int(math.log2(max(1, infos[i][1])))}" for i in range(nc)]
+    todo = [i for i in range(nc) if infos[i][1] > 0 and keys[i] not in cache]
+    timings = {}
+    for variant in (0, 1):
+        ok = []
+        for i in todo:
+            try:
+                fb.set_class_variant(i, variant)
+                ok.append(i)
+            except Exception:
+                pass
+        best = [math.inf] * nc
+        for _ in range(repeats):
+            ms = fb.profile_build(D_ptr, J_ptr, K_ptr)
+            for i in ok:
+                best[i] = min(best[i], ms[i])
+        for i in ok:
+            timings.setdefault(i, {})[variant] = best[i]
+    choice = {}
+    for i in range(nc):
+        if infos[i][1] == 0:
+            continue
+        if keys[i] in cache:
+            v = int(cache[keys[i]])
+        else:
+            t = timings.get(i, {0: 0.0})
+            v = min(t, key=t.get)
+            cache[keys[i]] = v
+        fb.set_class_variant(i, v)
+        choice[names[i]] = v
+    if cache_path:
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    return choice

@@ -33,9 +33,10 @@ CFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 
 def _classes(lmax: int):
     sys.path.insert(0, CSRC)
+    import gen_coop  # noqa: E402
     import gen_eri  # noqa: E402
 
-    return gen_eri.quartet_classes(lmax), gen_eri.pair_classes(lmax)
+    return gen_eri.quartet_classes(lmax), gen_eri.pair_classes(lmax), gen_coop.coop_classes(lmax)
 
 
 def _write_if_changed(path: str, text: str) -> None:
@@ -47,10 +48,10 @@ def _write_if_changed(path: str, text: str) -> None:
         f.write(text)
 
 
-def _class_tu(c) -> str:
+def _class_tu(c, coop: bool) -> str:
     la, lb, lc, ld = c
     name = f"{la}{lb}{lc}{ld}"
-    lines = [f'#include "eri_kernels.cuh"', ""]
+    lines = [f'#include "{"coop_kernels.cuh" if coop else "eri_kernels.cuh"}"', ""]
     lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, const EriArgs& a, cudaStream_t s) {{")
     lines.append("  const int threads = 128;")
     lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
@@ -72,11 +73,42 @@ def _class_tu(c) -> str:
                 lines.append(f"  if (boys == {boys} && pure == {pure}) "
                              f"schwarz_kernel<{la}, {lb}, {boys}, {pb}><<<blocks, threads, 0, s>>>(a);")
         lines.append("}")
+    if coop:
+        lines.append(f"void dss_launch_eri_coop_{name}(int boys, int pure, const EriArgs& a, cudaStream_t s) {{")
+        lines.append("  const unsigned blocks = (unsigned)((a.ntasks + DSS_COOP_WARPS - 1) / DSS_COOP_WARPS);")
+        lines.append("  if (!blocks) return;")
+        for boys in (0, 1):
+            for pure in (1, 0):
+                pb = "true" if pure else "false"
+                k = f"eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}>"
+                sm = f"coop_smem_per_warp<{la}, {lb}, {lc}, {ld}, {pb}>() * sizeof(double) * DSS_COOP_WARPS"
+                lines.append(f"  if (boys == {boys} && pure == {pure}) {{")
+                lines.append(f"    static bool attr = false;")
+                lines.append(f"    const size_t smem = {sm};")
+                lines.append(f"    if (!attr) {{ cudaFuncSetAttribute({k}, "
+                             f"cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }}")
+                lines.append(f"    {k}<<<blocks, 32 * DSS_COOP_WARPS, smem, s>>>(a);")
+                lines.append("  }")
+        lines.append("}")
     return "\n".join(lines) + "\n"
 
 
-def _dispatch_tu(classes, pcls) -> str:
+def _dispatch_tu(classes, pcls, coop) -> str:
     lines = ['#include "eri_kernels.cuh"', ""]
+    for (la, lb, lc, ld) in coop:
+        lines.append(f"void dss_launch_eri_coop_{la}{lb}{lc}{ld}(int boys, int pure, const EriArgs& a, cudaStream_t s);")
+    lines.append("bool dss_has_coop(int la, int lb, int lc, int ld) {")
+    for (la, lb, lc, ld) in coop:
+        lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) return true;")
+    lines.append("  return false;")
+    lines.append("}")
+    lines.append("void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant, "
+                 "const EriArgs& a, cudaStream_t s) {")
+    for (la, lb, lc, ld) in coop:
+        lines.append(f"  if (variant == 1 && la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
+                     f"return dss_launch_eri_coop_{la}{lb}{lc}{ld}(boys, pure, a, s);")
+    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, a, s);")
+    lines.append("}")
     for (la, lb) in pcls:
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s);")
     lines.append("void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s) {")
@@ -107,37 +139,49 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     eri_gen = os.path.join(GEN, "eri_gen.cuh")
     boys_tab = os.path.join(GEN, "boys_tab.cuh")
     gen_stamp = os.path.join(GEN, "stamp")
-    want = _stamp([os.path.join(CSRC, "gen_eri.py"), os.path.join(CSRC, "gen_boys_tab.py")], str(lmax))
+    want = _stamp([os.path.join(CSRC, "gen_eri.py"), os.path.join(CSRC, "gen_boys_tab.py"),
+                   os.path.join(CSRC, "gen_coop.py")], str(lmax))
     have = open(gen_stamp).read() if os.path.isfile(gen_stamp) else ""
     sph_tab = os.path.join(GEN, "sph_tab.h")
-    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, sph_tab)):
+    coop_gen = os.path.join(GEN, "coop_gen.cuh")
+    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, sph_tab, coop_gen)):
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_eri.py"), eri_gen, str(lmax)])
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_boys_tab.py"), boys_tab])
+        subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_coop.py"), coop_gen, str(lmax)])
         with open(gen_stamp, "w") as f:
             f.write(want)
-    classes, pcls = _classes(lmax)
+    classes, pcls, coop = _classes(lmax)
     units = []
     for c in classes:
         p = os.path.join(GEN, "eri_class_%d%d%d%d.cu" % c)
-        _write_if_changed(p, _class_tu(c))
+        _write_if_changed(p, _class_tu(c, c in coop))
         units.append(p)
     p = os.path.join(GEN, "eri_dispatch.cu")
-    _write_if_changed(p, _dispatch_tu(classes, pcls))
+    _write_if_changed(p, _dispatch_tu(classes, pcls, coop))
     units.append(p)
     for name in sorted(os.listdir(CSRC)):
         if name.endswith(".cu"):
             units.append(os.path.join(CSRC, name))
     headers = [os.path.join(CSRC, n) for n in sorted(os.listdir(CSRC)) if n.endswith((".cuh", ".h"))]
-    headers += [eri_gen, boys_tab, sph_tab, os.path.join(INCLUDE, "dss.h")]
+    headers += [eri_gen, boys_tab, sph_tab, coop_gen, os.path.join(INCLUDE, "dss.h")]
     all_stamp = _stamp(headers, " ".join(CFLAGS + ARCH))
     # The generated class units only see the kernel headers.
     kernel_headers = [os.path.join(CSRC, n) for n in ("eri_kernels.cuh", "common.cuh", "boys.cuh")]
     kernel_stamp = _stamp(kernel_headers + [eri_gen, boys_tab], " ".join(CFLAGS + ARCH))
+    coop_stamp = _stamp(kernel_headers + [eri_gen, boys_tab, coop_gen, os.path.join(CSRC, "coop_kernels.cuh")],
+                        " ".join(CFLAGS + ARCH))
+    coop_units = {"eri_class_%d%d%d%d.cu" % c for c in coop}
 
     def compile_one(src: str) -> str:
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         stamp = obj + ".stamp"
-        hdr = kernel_stamp if os.path.basename(src).startswith("eri_class_") else all_stamp
+        base = os.path.basename(src)
+        if base in coop_units:
+            hdr = coop_stamp
+        elif base.startswith("eri_class_"):
+            hdr = kernel_stamp
+        else:
+            hdr = all_stamp
         key = hdr + _stamp([src], "")
         if os.path.isfile(obj) and os.path.isfile(stamp) and open(stamp).read() == key:
             return obj

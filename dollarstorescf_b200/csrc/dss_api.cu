@@ -448,6 +448,11 @@ int dss_build_tasks(dss_ctx* ctx) {
     ct.lb = ci.lb;
     ct.lc = ci.lc;
     ct.ld = ci.ld;
+    const size_t idx = ctx->tasks.size();
+    if (idx < ctx->class_variant.size() && ctx->class_variant[idx] >= 0)
+      ct.variant = ctx->class_variant[idx];
+    else
+      ct.variant = dss_has_coop(ci.la, ci.lb, ci.lc, ci.ld) ? 1 : 0;
     std::vector<int4> h;
     for (int ib = ctx->class_pair0[bc]; ib < ctx->class_pair1[bc]; ++ib) {
       const double Qb = Q[ib];
@@ -523,7 +528,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.K = Kacc;
     a.n = n;
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], st));
-    dss_launch_eri_jk(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, a, st);
+    dss_launch_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, ct.variant, a, st);
     DSS_CUDA(cudaGetLastError());
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], st));
   }
@@ -576,6 +581,27 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* sq, long long*
   if (pq) *pq = have ? ctx->tasks[i].prim_quartets : 0;
   if (wt) *wt = have ? ctx->tasks[i].ntasks : 0;
   return DSS_OK;
+}
+
+int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
+  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 1) return DSS_ERR_INVALID;
+  if (ctx->class_variant.size() < (size_t)DSS_N_QUARTET_CLASSES) ctx->class_variant.assign(DSS_N_QUARTET_CLASSES, -1);
+  static const int kL[][4] = {
+#define DSS_CLASS_L2(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_},
+      DSS_FOR_EACH_CLASS(DSS_CLASS_L2)
+#undef DSS_CLASS_L2
+  };
+  if (variant == 1 && !dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]))
+    return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: no warp-cooperative kernel for this class");
+  ctx->class_variant[i] = variant;
+  if ((size_t)i < ctx->tasks.size())
+    ctx->tasks[i].variant = variant >= 0 ? variant : (dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]) ? 1 : 0);
+  return DSS_OK;
+}
+
+int dss_get_class_variant(const dss_ctx* ctx, int i) {
+  if (!ctx || i < 0 || (size_t)i >= ctx->tasks.size()) return -1;
+  return ctx->tasks[i].variant;
 }
 
 int dss_kernels_per_build(const dss_ctx* ctx) {

@@ -62,6 +62,7 @@ struct BasisHost {
 struct ClassTasks {
   int la = 0, lb = 0, lc = 0, ld = 0;
   int ntasks = 0;
+  int variant = 0;  // 0: thread per quartet, 1: warp-cooperative
   long long shell_quartets = 0, prim_quartets = 0;
   DevBuf<int4> d_tasks;
 };
@@ -93,6 +94,7 @@ struct dss_ctx {
   std::vector<double> h_Q;
   std::vector<int> class_pair0, class_pair1;
   std::vector<ClassTasks> tasks;
+  std::vector<int> class_variant;  // per class: -1 default, 0 thread, 1 warp-cooperative
   long long n_shell_quartets = 0, n_prim_quartets = 0, n_warp_tasks = 0;
 
   // build scratch

@@ -226,4 +226,8 @@ DSS_FOR_EACH_CLASS(DSS_DECLARE_LAUNCHERS)
 #undef DSS_DECLARE_LAUNCHERS
 
 void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s);
+// variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class).
+void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant, const EriArgs& a,
+                            cudaStream_t s);
+bool dss_has_coop(int la, int lb, int lc, int ld);
 void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, const EriArgs& a, cudaStream_t s);

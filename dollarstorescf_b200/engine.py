@@ -112,6 +112,15 @@ class FockBuilder:
         self._check(self._L.dss_class_info(self._h, i, l4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return list(l4), a.value, b.value, c.value
 
+    def num_classes(self) -> int:
+        return int(self._L.dss_num_classes())
+
+    def set_class_variant(self, i: int, variant: int) -> None:
+        self._check(self._L.dss_set_class_variant(self._h, i, variant))
+
+    def class_variant(self, i: int) -> int:
+        return int(self._L.dss_get_class_variant(self._h, i))
+
     def kernels_per_build(self) -> int:
         return int(self._L.dss_kernels_per_build(self._h))
 

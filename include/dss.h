@@ -101,6 +101,14 @@ int dss_num_classes(void);
 int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* shell_quartets, long long* prim_quartets,
                    long long* warp_tasks);
 
+/* Kernel variant of class i: 0 one thread per shell quartet, 1 one warp per
+ * shell quartet (shared-memory programs; only for the classes compiled with it),
+ * -1 the library default.  Used by the autotuner; persists across bases. */
+int dss_set_class_variant(dss_ctx* ctx, int i, int variant);
+
+/* The variant class i currently runs with (-1 before a basis is set). */
+int dss_get_class_variant(const dss_ctx* ctx, int i);
+
 /* Kernel launches one dss_build_jk_device call enqueues. */
 int dss_kernels_per_build(const dss_ctx* ctx);
 

@@ -64,5 +64,19 @@ for p in "${pids[@]}"; do wait "$p"; done
 g++ $CXXFLAGS -I"$SHADOW" -c "$HERE/ref_harness.cpp" -o "$OBJDIR/ref_harness.o"
 g++ -shared -o "$OUT/libdssref.so" "$OBJDIR"/*.o "$BLAS" \
     -Wl,--disable-new-dtags -Wl,-rpath,"$BLASDIR" -Wl,-rpath-link,"$BLASDIR" -lpthread
+
+# The drop-in variant: the same reference objects with chem/scf/ExactCoulomb.cpp
+# replaced by the engine's shim (dollarstorescf_b200/shim/ExactCoulomb_gpu.cpp),
+# linked against the engine library.  Used by the GPU drop-in test only.
+DSS_PKG="$(cd "$HERE/.." && pwd)/dollarstorescf_b200"
+if [ -f "$DSS_PKG/libdss.so" ]; then
+  g++ $CXXFLAGS -I"$SHADOW" -I"$(cd "$HERE/.." && pwd)/include" -c "$DSS_PKG/shim/ExactCoulomb_gpu.cpp" \
+      -o "$SHADOW/ExactCoulomb_gpu.o"
+  g++ -shared -o "$OUT/libdssref_gpu.so" $(ls "$OBJDIR"/*.o | grep -v chem_scf_ExactCoulomb.cpp.o) \
+      "$SHADOW/ExactCoulomb_gpu.o" "$BLAS" "$DSS_PKG/libdss.so" \
+      -Wl,--disable-new-dtags -Wl,-rpath,"$BLASDIR" -Wl,-rpath-link,"$BLASDIR" \
+      -Wl,-rpath,'$ORIGIN/../../dollarstorescf_b200' -lpthread
+  echo "built $OUT/libdssref_gpu.so"
+fi
 rm -rf "$SHADOW"
 echo "built $OUT/libdssref.so"

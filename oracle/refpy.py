@@ -12,7 +12,7 @@ from typing import Optional, Tuple
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_ref", "libdssref.so")
+LIB_PATH = os.path.join(HERE, "_ref", os.environ.get("DSS_REF_LIB", "libdssref.so"))
 
 _lib = None
 

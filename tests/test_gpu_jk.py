@@ -88,3 +88,26 @@ def test_errors_are_reported_not_fatal(builders):
     with pytest.raises(DssError, match="above the compiled maximum"):
         fb.set_basis(sh)
     fb.close()
+
+
+@pytest.mark.parametrize("name", ["dimer_631gs", "dimer_631gs_6d"])
+def test_kernel_variants_agree(builders, name):
+    # Every class through the thread-per-quartet kernel and, where compiled,
+    # the warp-cooperative one: both must reproduce the reference.
+    d, mol, sh = load_case(name)
+    fb = builders[BOYS_REF]
+    fb.set_basis(sh)
+    n = fb.num_classes()
+    results = []
+    for variant in (0, 1):
+        for i in range(n):
+            try:
+                fb.set_class_variant(i, variant)
+            except Exception:
+                fb.set_class_variant(i, 0)
+        J, K = fb.jk(2.0 * d["D_rand"])
+        assert np.abs(J - d["J_rand"]).max() < 1e-10
+        assert np.abs(0.5 * K - d["K_rand"]).max() < 1e-10
+        results.append((J, K))
+    for i in range(n):
+        fb.set_class_variant(i, -1)
