@@ -89,6 +89,8 @@ def load():
     L.dss_set_class_variant.restype = ctypes.c_int
     L.dss_get_class_variant.argtypes = [vp, ctypes.c_int]
     L.dss_get_class_variant.restype = ctypes.c_int
+    L.dss_eval_boys.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp]
+    L.dss_eval_boys.restype = ctypes.c_int
     L.dss_one_electron.argtypes = [vp, ctypes.c_int, ip, dp, dp, dp, dp, dp]
     L.dss_one_electron.restype = ctypes.c_int
     L.dss_default_scf_opts.argtypes = [ctypes.POINTER(DssScfOpts)]

@@ -75,7 +75,8 @@ def _class_tu(c, coop: bool) -> str:
         lines.append("}")
     if coop:
         lines.append(f"void dss_launch_eri_coop_{name}(int boys, int pure, const EriArgs& a, cudaStream_t s) {{")
-        lines.append("  const unsigned blocks = (unsigned)((a.ntasks + DSS_COOP_WARPS - 1) / DSS_COOP_WARPS);")
+        lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * DSS_COOP_SPLIT + DSS_COOP_WARPS - 1) / "
+                     "DSS_COOP_WARPS);")
         lines.append("  if (!blocks) return;")
         for boys in (0, 1):
             for pure in (1, 0):

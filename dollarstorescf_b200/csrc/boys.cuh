@@ -54,7 +54,7 @@ __device__ __forceinline__ double ref_ipow(double x, unsigned p) {
 }
 
 template <int L>
-__device__ __forceinline__ void boys_ref(double x, double* F) {
+__device__ __forceinline__ void boys_ref_series(double x, double* F) {
   const double ex = exp(-x);
   // m values with x > 1.1 m + 25 take the asymptotic branch; they are the lowest m.
   // Series for the remaining m are built from the top down.
@@ -160,6 +160,106 @@ __device__ __forceinline__ void boys_fast(double x, double* F) {
     F[0] = 0.5 * sqrt(3.141592653589793 / x);
 #pragma unroll
     for (int m = 0; m < L; ++m) F[m + 1] = ((double)(2 * m + 1) * F[m] - ex) * inv2x;
+  }
+}
+
+// Reference-mode Boys without running the series.  The m = L series the
+// reference would sum is  S = sum_{i<=n} t_i,  t_i = (2x)^i / prod_{j<=i}(2L+2j+1),
+// stopped at n = first i >= 1 with t_i <= 1e-9.  Then
+//   S = e^x (2L+1) F_L(x) - sum_{i>n} t_i,
+// with F_L from the accurate table (boys_fast), n from the tabulated truncation
+// breakpoints (n = 1 + #{k : B_L[k] < x}, boys_tab.cuh), t_n = exp(n ln 2x - LP_L[n])
+// and the short geometric tail summed directly.  The lower orders follow by the
+// same truncation-adjusting downward step as boys_ref_series.  When x lies within
+// a relative 4e-14 of a breakpoint (where rounding decides the reference's stop),
+// or L exceeds the tables, the series itself runs.
+template <int L>
+__device__ __forceinline__ void boys_ref(double x, double* F) {
+  int m_series_lo = L + 1;
+#pragma unroll
+  for (int m = L; m >= 0; --m) {
+    const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
+    if (!(x > thr)) m_series_lo = m;
+  }
+  if (L >= DSS_BOYS_NLB || m_series_lo > L || !(x > 1e-280) || !(x < 35.9)) {
+    boys_ref_series<L>(x, F);
+    return;
+  }
+  // Truncation index of the m = L series.
+  const double* bp = g_boys_bp + L * (DSS_BOYS_NB + 1);
+  int n = 1 + (int)g_boys_idx[L * DSS_BOYS_NG + (int)(x * 4.0)];
+  while (n <= DSS_BOYS_NB && bp[n] < x) ++n;
+  if (n > DSS_BOYS_NB) {
+    boys_ref_series<L>(x, F);
+    return;
+  }
+  const double lo_b = bp[n - 1], hi_b = bp[n];  // lo_b < x <= hi_b (bp[0] = 0)
+  if (fabs(x - hi_b) <= 4e-14 * x || fabs(x - lo_b) <= 4e-14 * x) {
+    boys_ref_series<L>(x, F);
+    return;
+  }
+  // Accurate F_L (7-term Taylor about the nearest table point).
+  const int k = __double2int_rn(x * (double)DSS_BOYS_STEP);
+  const double dx = (double)k * (1.0 / DSS_BOYS_STEP) - x;
+  const double* row = g_boys_tab + k * DSS_BOYS_NM + L;
+  double fl = row[6] * (1.0 / 720.0);
+  fl = fl * dx + row[5] * (1.0 / 120.0);
+  fl = fl * dx + row[4] * (1.0 / 24.0);
+  fl = fl * dx + row[3] * (1.0 / 6.0);
+  fl = fl * dx + row[2] * 0.5;
+  fl = fl * dx + row[1];
+  fl = fl * dx + row[0];
+  const double ex = exp(-x);
+  const double x2 = 2.0 * x;
+  const double tn = exp((double)n * log(x2) - g_boys_lp[L * (DSS_BOYS_NB + 1) + n]);
+  double tail = 0.0, t = tn;
+  for (int j = 1; j <= 64; ++j) {
+    t = t * x2 * odd_inv(L + n + j);
+    tail += t;
+    if (t < 1e-32) break;
+  }
+  double S = fl * (double)(2 * L + 1) / ex - tail;
+  double last = tn;
+  F[L] = fl - ex * tail * odd_inv(L);
+#pragma unroll
+  for (int m = L - 1; m >= 0; --m) {
+    if (m < m_series_lo) break;
+    const double c = 2.0 * x * odd_inv(m + 1);
+    double Sm1 = S, tt = last;
+    int kk = n;
+    if (c * tt <= 0.000000001) {
+      while (kk > 0) {
+        const double tp = tt * (double)(2 * (m + 1) + 2 * kk + 1) / x2;
+        if (c * tp <= 0.000000001) {
+          Sm1 -= tt;
+          tt = tp;
+          --kk;
+        } else {
+          break;
+        }
+      }
+    } else {
+      do {
+        tt = tt * x2 * odd_inv(m + 1 + kk + 1);
+        Sm1 += tt;
+        ++kk;
+      } while (c * tt > 0.000000001);
+    }
+    S = 1.0 + c * Sm1;
+    last = c * tt;
+    n = kk + 1;
+    F[m] = ex * odd_inv(m) * S;
+  }
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if (m < m_series_lo) {
+      unsigned int dfi = 1u;
+      for (int j = 2 * m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
+      const double df = (double)(int)dfi;
+      double p2 = 1.0;
+      for (int j = 0; j < m + 1; ++j) p2 *= 2.0;
+      F[m] = df / p2 * sqrt(DSS_PI_REF / ref_ipow(x, 2 * m + 1));
+    }
   }
 }
 

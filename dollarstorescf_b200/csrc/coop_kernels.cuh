@@ -1,7 +1,7 @@
 // Warp-cooperative ERI + J/K digest for the high-angular-momentum classes.
 //
-// One warp evaluates one shell quartet at a time (the kets of its warp task in
-// turn).  The recurrences are the same as the thread-per-quartet kernels but
+// One warp evaluates one shell quartet: warp task t (one bra pair, up to 32 kets)
+// is spread over DSS_COOP_SPLIT warps, one ket each.  The recurrences are the same as the thread-per-quartet kernels but
 // run as the generated operation programs of coop_gen.cuh over a per-warp
 // shared-memory value array: the VRR program once per primitive quartet
 // (accumulating into the contracted [e0|f0]), then the HRR + function-transform
@@ -14,8 +14,9 @@
 #include "coop_gen.cuh"
 #include "eri_kernels.cuh"
 
-#define DSS_COOP_WARPS 4
-#define DSS_COOP_BATCH 8
+#define DSS_COOP_WARPS 1   // warps per block: small blocks let shared memory set occupancy
+#define DSS_COOP_SPLIT 32  // warps per warp task: each warp takes one ket of the task
+#define DSS_COOP_BATCH 8   // primitive-quartet records prepared per pass
 
 template <int LA, int LB, int LC, int LD, bool PURE>
 struct CoopProg;
@@ -81,7 +82,9 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
   extern __shared__ double smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int warp = blockIdx.x * DSS_COOP_WARPS + wib;
+  const long long gw = (long long)blockIdx.x * DSS_COOP_WARPS + wib;
+  const int warp = (int)(gw / DSS_COOP_SPLIT);
+  const int part = (int)(gw % DSS_COOP_SPLIT);
   if (warp >= a.ntasks) return;  // uniform per warp
   double* vals = smem + PER_WARP * wib;
   double* recs = vals + P::NSLOTS;
@@ -95,6 +98,9 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
   double* dbc = dac + NA * NC;
 
   const int4 t = __ldg(a.tasks + warp);
+  const int k_begin = part * ((t.z + DSS_COOP_SPLIT - 1) / DSS_COOP_SPLIT);
+  const int k_end = min(t.z, k_begin + (t.z + DSS_COOP_SPLIT - 1) / DSS_COOP_SPLIT);
+  if (k_begin >= k_end) return;  // uniform per warp
   const int bra = t.x;
   const int sa = __ldg(a.pair_a + bra), sb = __ldg(a.pair_b + bra);
   const int n = a.n;
@@ -113,7 +119,7 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
   const double* __restrict__ wts = P::w();
   const unsigned short* __restrict__ outs = P::out();
 
-  for (int kq = 0; kq < t.z; ++kq) {
+  for (int kq = k_begin; kq < k_end; ++kq) {
     const int ket = t.y + kq;
     const int sc = __ldg(a.pair_a + ket), sd = __ldg(a.pair_b + ket);
     const int fc = __ldg(a.sh_f0 + sc), fd = __ldg(a.sh_f0 + sd);
@@ -142,9 +148,9 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
       for (int j = 0; j < nb; ++j) {
         const double* __restrict__ r = recs + j * DSS_REC;
         for (int lv = 0; lv < P::NVLV; ++lv) {
-          const int o1 = vlv[lv + 1];
-          for (int o = vlv[lv] + lane; o < o1; o += 32) {
-            const uint4 op = vrr[o];
+          const int o1 = __ldg(vlv + lv + 1);
+          for (int o = __ldg(vlv + lv) + lane; o < o1; o += 32) {
+            const uint4 op = __ldg(vrr + o);
             const unsigned dst = op.x & 0xFFFFu, s0 = op.x >> 16, s1 = op.y & 0xFFFFu, s2 = op.y >> 16;
             const unsigned s3 = op.z & 0xFFFFu, s4 = op.z >> 16;
             const unsigned kind = op.w & 15u, ax = (op.w >> 4) & 3u;
@@ -163,7 +169,7 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
           __syncwarp();
         }
         for (int o = lane; o < P::NACC; o += 32) {
-          const uint4 op = accp[o];
+          const uint4 op = __ldg(accp + o);
           vals[(op.x & 0xFFFFu) - 32u] += coop_get(r, vals, op.x >> 16);
         }
         __syncwarp();
@@ -171,9 +177,9 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
     }
     // HRR + transform
     for (int lv = 0; lv < P::NHLV; ++lv) {
-      const int o1 = hlv[lv + 1];
-      for (int o = hlv[lv] + lane; o < o1; o += 32) {
-        const uint4 op = hrr[o];
+      const int o1 = __ldg(hlv + lv + 1);
+      for (int o = __ldg(hlv + lv) + lane; o < o1; o += 32) {
+        const uint4 op = __ldg(hrr + o);
         const unsigned dst = op.x & 0xFFFFu, s0 = op.x >> 16, s1 = op.y & 0xFFFFu, s2 = op.y >> 16;
         const unsigned kind = op.w & 15u;
         double v;
@@ -181,9 +187,9 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
           const unsigned ax = (op.w >> 4) & 3u, side = (op.w >> 6) & 1u;
           v = vals[s0 - 32u] + hdr[3 * side + ax] * vals[s1 - 32u];
         } else {
-          v = wts[op.z & 0xFFFFu] * vals[s0 - 32u];
-          if (s1 != 0xFFFFu) v += wts[op.z >> 16] * vals[s1 - 32u];
-          if (s2 != 0xFFFFu) v += wts[op.w >> 16] * vals[s2 - 32u];
+          v = __ldg(wts + (op.z & 0xFFFFu)) * vals[s0 - 32u];
+          if (s1 != 0xFFFFu) v += __ldg(wts + (op.z >> 16)) * vals[s1 - 32u];
+          if (s2 != 0xFFFFu) v += __ldg(wts + (op.w >> 16)) * vals[s2 - 32u];
         }
         vals[dst - 32u] = v;
       }
@@ -200,7 +206,7 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
     for (int q = lane; q < NA * NC; q += 32) dac[q] = __ldg(a.D + (size_t)(fa + q / NC) * n + fc + q % NC);
     for (int q = lane; q < NB * NC; q += 32) dbc[q] = __ldg(a.D + (size_t)(fb + q / NC) * n + fc + q % NC);
     __syncwarp();
-#define DSS_I(i, j, k, l) vals[outs[(((i) * NB + (j)) * NC + (k)) * ND + (l)] - 32u]
+#define DSS_I(i, j, k, l) vals[__ldg(outs + (((i) * NB + (j)) * NC + (k)) * ND + (l)) - 32u]
     // J over the bra pair: accumulated in shared memory across the task's kets.
     for (int q = lane; q < NA * NB; q += 32) {
       const int i = q / NB, j = q % NB;

@@ -665,3 +665,43 @@ int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ Boys check
+#include "boys.cuh"
+namespace {
+template <int L>
+__global__ void boys_check_kernel(int mode, const double* x, int n, double* F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double f[L + 1];
+  if (mode == DSS_BOYS_REF) boys_ref<L>(x[i], f);
+  else if (mode == DSS_BOYS_FAST) boys_fast<L>(x[i], f);
+  else boys_ref_series<L>(x[i], f);
+  for (int m = 0; m <= L; ++m) F[(size_t)i * (L + 1) + m] = f[m];
+}
+}  // namespace
+
+extern "C" int dss_eval_boys(dss_ctx* ctx, int mode, int L, const double* x, int n, double* F) {
+  if (!ctx || !x || !F || n < 0 || L < 0 || L > 12 || mode < 0 || mode > 2) return DSS_ERR_INVALID;
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  DevBuf<double> dx, dF;
+  DSS_CUDA(dx.resize(n > 0 ? n : 1));
+  DSS_CUDA(dF.resize((size_t)(n > 0 ? n : 1) * (L + 1)));
+  DSS_CUDA(cudaMemcpyAsync(dx.ptr, x, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  const unsigned blocks = (unsigned)((n + 127) / 128);
+  if (n > 0) {
+    switch (L) {
+#define DSS_BC(l)                                                                    \
+  case l:                                                                            \
+    boys_check_kernel<l><<<blocks, 128, 0, ctx->stream>>>(mode, dx.ptr, n, dF.ptr); \
+    break;
+      DSS_BC(0) DSS_BC(1) DSS_BC(2) DSS_BC(3) DSS_BC(4) DSS_BC(5) DSS_BC(6) DSS_BC(7) DSS_BC(8) DSS_BC(9)
+      DSS_BC(10) DSS_BC(11) DSS_BC(12)
+#undef DSS_BC
+    }
+  }
+  DSS_CUDA(cudaGetLastError());
+  DSS_CUDA(cudaMemcpyAsync(F, dF.ptr, (size_t)n * (L + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  DSS_CUDA(cudaStreamSynchronize(ctx->stream));
+  return DSS_OK;
+}

@@ -31,6 +31,37 @@ def main() -> None:
         for i in range(0, len(vals), 4):
             f.write("  " + ", ".join(repr(v) for v in vals[i:i + 4]) + ",\n")
         f.write("};\n")
+        # Truncation breakpoints of the reference's series (boys.cuh, boys_ref):
+        # for order L the m=L series stops at the first n >= 1 with
+        # t_n = (2x)^n / prod_{j=1..n}(2L+2j+1) <= 1e-9, i.e. at n(x) = 1 + #{k >= 1 : B_L[k] < x}
+        # with B_L[k] = 0.5 exp((ln 1e-9 + LP_L[k]) / k), LP_L[k] = sum_{j=1..k} ln(2L+2j+1).
+        NLB, NB = 16, 160
+        mpmath.mp.dps = 40
+        LP = [[0.0] * (NB + 1) for _ in range(NLB)]
+        BP = [[0.0] * (NB + 1) for _ in range(NLB)]
+        for L in range(NLB):
+            acc = mpmath.mpf(0)
+            prev = mpmath.mpf(-1)
+            for k in range(1, NB + 1):
+                acc += mpmath.log(2 * L + 2 * k + 1)
+                LP[L][k] = float(acc)
+                b = mpmath.mpf("0.5") * mpmath.exp((mpmath.log(mpmath.mpf("1e-9")) + acc) / k)
+                assert b > prev, (L, k)
+                prev = b
+                BP[L][k] = float(b)
+        # Coarse index: for x in [g/4, (g+1)/4): the count of breakpoints below g/4.
+        NG = 200
+        IDX = [[sum(1 for k in range(1, NB + 1) if BP[L][k] < g / 4.0) for g in range(NG)] for L in range(NLB)]
+        f.write(f"#define DSS_BOYS_NLB {NLB}\n#define DSS_BOYS_NB {NB}\n#define DSS_BOYS_NG {NG}\n")
+        for name, tab in (("g_boys_bp", BP), ("g_boys_lp", LP)):
+            f.write("static __device__ const double %s[%d] = {\n" % (name, NLB * (NB + 1)))
+            for L in range(NLB):
+                f.write("  " + ", ".join(repr(v) for v in tab[L]) + ",\n")
+            f.write("};\n")
+        f.write("static __device__ const unsigned char g_boys_idx[%d] = {\n" % (NLB * NG))
+        for L in range(NLB):
+            f.write("  " + ", ".join(str(v) for v in IDX[L]) + ",\n")
+        f.write("};\n")
         f.write("static __device__ const double g_odd_inv[256] = {\n")
         inv = [1.0 / (2 * k + 1) for k in range(256)]
         for i in range(0, 256, 4):

@@ -112,6 +112,12 @@ class FockBuilder:
         self._check(self._L.dss_class_info(self._h, i, l4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return list(l4), a.value, b.value, c.value
 
+    def eval_boys(self, mode: int, L: int, x: np.ndarray) -> np.ndarray:
+        xs = np.ascontiguousarray(x, dtype=np.float64)
+        F = np.empty((xs.size, L + 1))
+        self._check(self._L.dss_eval_boys(self._h, mode, L, _dp(xs), xs.size, _dp(F)))
+        return F
+
     def num_classes(self) -> int:
         return int(self._L.dss_num_classes())
 

@@ -118,6 +118,12 @@ int dss_kernels_per_build(const dss_ctx* ctx);
 int dss_profile_build(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev,
                       float* ms_per_class);
 
+/* Device Boys function F_0..F_L (L <= 12) at n points x[] into F[n*(L+1)]:
+ * mode DSS_BOYS_REF (the reference's truncated series, evaluated from the
+ * accurate function and the tabulated truncation points), DSS_BOYS_FAST, or 2
+ * (the reference's series summed term by term).  For tests and diagnostics. */
+int dss_eval_boys(dss_ctx* ctx, int mode, int L, const double* x, int n, double* F);
+
 /* Measures the device's double-precision FMA throughput with a register-only
  * loop (the FP64 CUDA-core roofline the ERI kernels are reported against). */
 int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops);
