@@ -25,7 +25,9 @@ class DssError(RuntimeError):
 
 class DssScfOpts(ctypes.Structure):
     _fields_ = [("conv", ctypes.c_double), ("diis_size", ctypes.c_int), ("max_iter", ctypes.c_int),
-                ("use_guess", ctypes.c_int)]
+                ("use_guess", ctypes.c_int), ("incremental", ctypes.c_int), ("fp32_threshold", ctypes.c_double),
+                ("skip_threshold", ctypes.c_double), ("rebuild_every", ctypes.c_int),
+                ("final_switch", ctypes.c_double)]
 
 
 class DssOpts(ctypes.Structure):
@@ -91,6 +93,8 @@ def load():
     L.dss_get_class_variant.restype = ctypes.c_int
     L.dss_eval_boys.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp]
     L.dss_eval_boys.restype = ctypes.c_int
+    L.dss_build_jk_mixed_device.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double]
+    L.dss_build_jk_mixed_device.restype = ctypes.c_int
     L.dss_one_electron.argtypes = [vp, ctypes.c_int, ip, dp, dp, dp, dp, dp]
     L.dss_one_electron.restype = ctypes.c_int
     L.dss_default_scf_opts.argtypes = [ctypes.POINTER(DssScfOpts)]

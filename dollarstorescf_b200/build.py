@@ -49,18 +49,22 @@ def _write_if_changed(path: str, text: str) -> None:
 
 
 def _class_tu(c, coop: bool) -> str:
+    """One translation unit per class: its kernels and host launchers.
+    Variants: Boys mode (0 reference, 1 accurate) x 5D/6D, plus the
+    mixed-precision screened form with the accurate Boys function."""
     la, lb, lc, ld = c
     name = f"{la}{lb}{lc}{ld}"
     lines = [f'#include "{"coop_kernels.cuh" if coop else "eri_kernels.cuh"}"', ""]
-    lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, const EriArgs& a, cudaStream_t s) {{")
+    combos = [(0, 1, 0), (0, 0, 0), (1, 1, 0), (1, 0, 0), (1, 1, 1), (1, 0, 1)]
+    lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, const EriArgs& a, cudaStream_t s) {{")
     lines.append("  const int threads = 128;")
     lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
     lines.append("  if (!blocks) return;")
-    for boys in (0, 1):
-        for pure in (1, 0):
-            pb = "true" if pure else "false"
-            lines.append(f"  if (boys == {boys} && pure == {pure}) "
-                         f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}><<<blocks, threads, 0, s>>>(a);")
+    for boys, pure, mixed in combos:
+        pb = "true" if pure else "false"
+        mb = "true" if mixed else "false"
+        lines.append(f"  if (boys == {boys} && pure == {pure} && mixed == {mixed}) "
+                     f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}><<<blocks, threads, 0, s>>>(a);")
     lines.append("}")
     if (la, lb) == (lc, ld):
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s) {{")
@@ -74,22 +78,23 @@ def _class_tu(c, coop: bool) -> str:
                              f"schwarz_kernel<{la}, {lb}, {boys}, {pb}><<<blocks, threads, 0, s>>>(a);")
         lines.append("}")
     if coop:
-        lines.append(f"void dss_launch_eri_coop_{name}(int boys, int pure, const EriArgs& a, cudaStream_t s) {{")
+        lines.append(f"void dss_launch_eri_coop_{name}(int boys, int pure, int mixed, const EriArgs& a, "
+                     f"cudaStream_t s) {{")
         lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * DSS_COOP_SPLIT + DSS_COOP_WARPS - 1) / "
                      "DSS_COOP_WARPS);")
         lines.append("  if (!blocks) return;")
-        for boys in (0, 1):
-            for pure in (1, 0):
-                pb = "true" if pure else "false"
-                k = f"eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}>"
-                sm = f"coop_smem_per_warp<{la}, {lb}, {lc}, {ld}, {pb}>() * sizeof(double) * DSS_COOP_WARPS"
-                lines.append(f"  if (boys == {boys} && pure == {pure}) {{")
-                lines.append(f"    static bool attr = false;")
-                lines.append(f"    const size_t smem = {sm};")
-                lines.append(f"    if (!attr) {{ cudaFuncSetAttribute({k}, "
-                             f"cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }}")
-                lines.append(f"    {k}<<<blocks, 32 * DSS_COOP_WARPS, smem, s>>>(a);")
-                lines.append("  }")
+        for boys, pure, mixed in combos:
+            pb = "true" if pure else "false"
+            mb = "true" if mixed else "false"
+            k = f"eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}>"
+            sm = f"coop_smem_per_warp<{la}, {lb}, {lc}, {ld}, {pb}>() * sizeof(double) * DSS_COOP_WARPS"
+            lines.append(f"  if (boys == {boys} && pure == {pure} && mixed == {mixed}) {{")
+            lines.append(f"    static bool attr = false;")
+            lines.append(f"    const size_t smem = {sm};")
+            lines.append(f"    if (!attr) {{ cudaFuncSetAttribute({k}, "
+                         f"cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }}")
+            lines.append(f"    {k}<<<blocks, 32 * DSS_COOP_WARPS, smem, s>>>(a);")
+            lines.append("  }")
         lines.append("}")
     return "\n".join(lines) + "\n"
 
@@ -97,18 +102,19 @@ def _class_tu(c, coop: bool) -> str:
 def _dispatch_tu(classes, pcls, coop) -> str:
     lines = ['#include "eri_kernels.cuh"', ""]
     for (la, lb, lc, ld) in coop:
-        lines.append(f"void dss_launch_eri_coop_{la}{lb}{lc}{ld}(int boys, int pure, const EriArgs& a, cudaStream_t s);")
+        lines.append(f"void dss_launch_eri_coop_{la}{lb}{lc}{ld}(int boys, int pure, int mixed, const EriArgs& a, "
+                     f"cudaStream_t s);")
     lines.append("bool dss_has_coop(int la, int lb, int lc, int ld) {")
     for (la, lb, lc, ld) in coop:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) return true;")
     lines.append("  return false;")
     lines.append("}")
-    lines.append("void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant, "
+    lines.append("void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int variant, "
                  "const EriArgs& a, cudaStream_t s) {")
     for (la, lb, lc, ld) in coop:
         lines.append(f"  if (variant == 1 && la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
-                     f"return dss_launch_eri_coop_{la}{lb}{lc}{ld}(boys, pure, a, s);")
-    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, a, s);")
+                     f"return dss_launch_eri_coop_{la}{lb}{lc}{ld}(boys, pure, mixed, a, s);")
+    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, mixed, a, s);")
     lines.append("}")
     for (la, lb) in pcls:
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s);")
@@ -116,11 +122,11 @@ def _dispatch_tu(classes, pcls, coop) -> str:
     for (la, lb) in pcls:
         lines.append(f"  if (la == {la} && lb == {lb}) return dss_launch_schwarz_{la}{lb}(boys, pure, a, s);")
     lines.append("}")
-    lines.append("void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, const EriArgs& a, "
-                 "cudaStream_t s) {")
+    lines.append("void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, "
+                 "const EriArgs& a, cudaStream_t s) {")
     for (la, lb, lc, ld) in classes:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
-                     f"return dss_launch_eri_jk_{la}{lb}{lc}{ld}(boys, pure, a, s);")
+                     f"return dss_launch_eri_jk_{la}{lb}{lc}{ld}(boys, pure, mixed, a, s);")
     lines.append("}")
     return "\n".join(lines) + "\n"
 

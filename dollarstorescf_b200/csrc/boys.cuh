@@ -135,6 +135,7 @@ __device__ __forceinline__ void boys_ref_series(double x, double* F) {
 
 template <int L>
 __device__ __forceinline__ void boys_fast(double x, double* F) {
+  static_assert(L + 6 < DSS_BOYS_NM, "Boys table too narrow for this order");
   if (x < 35.9) {
     const int k = __double2int_rn(x * (double)DSS_BOYS_STEP);
     const double dx = (double)k * (1.0 / DSS_BOYS_STEP) - x;  // x0 - x
@@ -181,7 +182,7 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
     const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
     if (!(x > thr)) m_series_lo = m;
   }
-  if (L >= DSS_BOYS_NLB || m_series_lo > L || !(x > 1e-280) || !(x < 35.9)) {
+  if (L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || m_series_lo > L || !(x > 1e-280) || !(x < 35.9)) {
     boys_ref_series<L>(x, F);
     return;
   }

@@ -72,7 +72,7 @@ __host__ __device__ constexpr size_t coop_smem_per_warp() {
          (NA * NB) * 2 + NC * ND + NA * ND + NB * ND + NA * NC + NB * NC;
 }
 
-template <int LA, int LB, int LC, int LD, int BOYS, bool PURE>
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false>
 __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a) {
   using P = CoopProg<LA, LB, LC, LD, PURE>;
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
@@ -125,6 +125,9 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
     const int fc = __ldg(a.sh_f0 + sc), fd = __ldg(a.sh_f0 + sd);
     const PrimPair* kpp = a.pp + __ldg(a.pair_pp0 + ket);
     const int nkp = __ldg(a.pair_npp + ket);
+    if constexpr (MIXED) {  // uniform across the warp
+      if (__ldg(a.Qp + bra) * __ldg(a.Qp + ket) * quartet_dbound(a, sa, sb, sc, sd) < a.skip_thr) continue;
+    }
     if (lane < 6) {
       const int s0 = lane < 3 ? sa : sc, s1 = lane < 3 ? sb : sd, ax = lane % 3;
       hdr[lane] = __ldg(a.sh_xyz + 3 * s0 + ax) - __ldg(a.sh_xyz + 3 * s1 + ax);

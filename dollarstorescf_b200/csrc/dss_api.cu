@@ -403,6 +403,13 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
   if ((rc = upload(ctx, ctx->d_pair_b, pb2)) != DSS_OK) return rc;
   if ((rc = upload(ctx, ctx->d_pair_pp0, p02)) != DSS_OK) return rc;
   if ((rc = upload(ctx, ctx->d_pair_npp, pn2)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_Qs, Q2)) != DSS_OK) return rc;
+  {
+    std::vector<int> nf(ctx->nshell);
+    for (int q = 0; q < ctx->nshell; ++q) nf[q] = ctx->basis.pure ? 2 * ctx->basis.l[q] + 1
+                                                                  : (ctx->basis.l[q] + 1) * (ctx->basis.l[q] + 2) / 2;
+    if ((rc = upload(ctx, ctx->d_sh_nf, nf)) != DSS_OK) return rc;
+  }
   ctx->h_pair_a = pa2;
   ctx->h_pair_b = pb2;
   ctx->h_pair_npp = pn2;
@@ -488,7 +495,11 @@ int dss_build_tasks(dss_ctx* ctx) {
   return DSS_OK;
 }
 
-int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events) {
+int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events,
+                   const BuildMode* mode) {
+  BuildMode def;
+  def.boys = ctx->opts.boys_mode;
+  if (!mode) mode = &def;
   const int n = ctx->nbf;
   const size_t nn = (size_t)n * n;
   DSS_CUDA(cudaMemsetAsync(Jacc, 0, nn * sizeof(double), ctx->stream));
@@ -527,8 +538,14 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.J = Jacc;
     a.K = Kacc;
     a.n = n;
+    a.Qp = ctx->d_Qs.ptr;
+    a.dmax = mode->dmax;
+    a.ns = ctx->nshell;
+    a.skip_thr = mode->skip_thr;
+    a.fp32_thr = mode->fp32_thr;
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], st));
-    dss_launch_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, ct.variant, a, st);
+    dss_launch_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, mode->mixed ? DSS_BOYS_FAST : mode->boys, ctx->pure,
+                           mode->mixed, ct.variant, a, st);
     DSS_CUDA(cudaGetLastError());
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], st));
   }
@@ -539,6 +556,25 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     }
   }
   return DSS_OK;
+}
+
+namespace {
+__global__ void block_max_kernel(const double* __restrict__ D, int n, const int* __restrict__ f0,
+                                 const int* __restrict__ nf, int ns, float* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns * ns) return;
+  const int a = t / ns, b = t % ns;
+  double m = 0.0;
+  for (int i = 0; i < nf[a]; ++i)
+    for (int j = 0; j < nf[b]; ++j) m = fmax(m, fabs(D[(size_t)(f0[a] + i) * n + f0[b] + j]));
+  out[t] = (float)(m * (1.0 + 1e-6));  // round up: the bound stays a bound in float
+}
+}  // namespace
+
+void dss_block_max(dss_ctx* ctx, const double* D, float* dmax) {
+  const int ns = ctx->nshell;
+  block_max_kernel<<<(ns * ns + 255) / 256, 256, 0, ctx->stream>>>(D, ctx->nbf, ctx->d_sh_f0.ptr,
+                                                                    ctx->d_sh_nf.ptr, ns, dmax);
 }
 
 namespace {
@@ -556,6 +592,34 @@ __global__ void fp64_probe_kernel(double* out, int iters, double b, double c) {
 }  // namespace
 
 extern "C" {
+
+int dss_build_jk_mixed_device(dss_ctx* ctx, const double* D, double* J, double* K, double fp32_threshold,
+                              double skip_threshold) {
+  if (!ctx) return DSS_ERR_INVALID;
+  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk_mixed_device: no basis set");
+  if (!D) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk_mixed_device: D is NULL");
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  const int n = ctx->nbf;
+  const size_t nn = (size_t)n * n;
+  DSS_CUDA(ctx->Jacc.resize(nn));
+  DSS_CUDA(ctx->Kacc.resize(nn));
+  DSS_CUDA(ctx->d_dmax.resize((size_t)ctx->nshell * ctx->nshell));
+  dss_block_max(ctx, D, ctx->d_dmax.ptr);
+  BuildMode m;
+  m.boys = DSS_BOYS_FAST;
+  m.mixed = 1;
+  m.dmax = ctx->d_dmax.ptr;
+  m.fp32_thr = fp32_threshold;
+  m.skip_thr = skip_threshold;
+  int rc = dss_enqueue_jk(ctx, D, ctx->Jacc.ptr, ctx->Kacc.ptr, nullptr, &m);
+  if (rc != DSS_OK) return rc;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((nn + threads - 1) / threads);
+  if (J) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Jacc.ptr, J, nullptr, n);
+  if (K) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Kacc.ptr, K, nullptr, n);
+  DSS_CUDA(cudaGetLastError());
+  return DSS_OK;
+}
 
 int dss_set_stream(dss_ctx* ctx, void* stream) {
   if (!ctx) return DSS_ERR_INVALID;

@@ -89,7 +89,9 @@ struct dss_ctx {
   BasisHost basis;
   DevBuf<PrimPair> d_pp;
   DevBuf<int> d_pair_a, d_pair_b, d_pair_pp0, d_pair_npp, d_sh_f0;
-  DevBuf<double> d_sh_xyz, d_Q;
+  DevBuf<double> d_sh_xyz, d_Q, d_Qs;  // Schwarz factors: computation order, sorted pair order
+  DevBuf<int> d_sh_nf;                  // functions per shell
+  DevBuf<float> d_dmax;
   std::vector<int> h_pair_a, h_pair_b, h_pair_npp, h_pair_cls;
   std::vector<double> h_Q;
   std::vector<int> class_pair0, class_pair1;
@@ -110,6 +112,9 @@ struct dss_ctx {
     d_sh_f0.free();
     d_sh_xyz.free();
     d_Q.free();
+    d_Qs.free();
+    d_sh_nf.free();
+    d_dmax.free();
     tasks.clear();
     nbf = 0;
   }
@@ -132,6 +137,18 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
 int dss_build_tasks(dss_ctx* ctx);
 // G = (Jacc + Jacc^T) - (Kacc + Kacc^T) / 2, dense n x n.
 void dss_symmetrize_combine(cudaStream_t s, int n, const double* Jacc, const double* Kacc, double* G);
+// How one J/K accumulation runs: Boys mode and, for the mixed-precision form,
+// the density-weighted screen (dmax: per shell block max |D|, device).
+struct BuildMode {
+  int boys = 0;
+  int mixed = 0;
+  const float* dmax = nullptr;
+  double skip_thr = 0.0, fp32_thr = 0.0;
+};
+
 // Enqueues one J/K accumulation; with events != NULL records events[2i], events[2i+1]
-// around the launch of class i.
-int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events = nullptr);
+// around the launch of class i.  mode == NULL: the context's Boys mode, FP64.
+int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events = nullptr,
+                   const BuildMode* mode = nullptr);
+// Per shell-pair block maximum of |D| (dense n x n, device) into dmax [nshell^2].
+void dss_block_max(dss_ctx* ctx, const double* D, float* dmax);

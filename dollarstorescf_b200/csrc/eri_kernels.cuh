@@ -36,6 +36,13 @@ struct EriArgs {
   double* J;              // dense n x n accumulators (Jacc, Kacc above)
   double* K;
   int n;
+  // Density-weighted screening (mixed-precision form only): a quartet is
+  // skipped when Q_ab Q_cd max|D| over its six density blocks is below skip_thr,
+  // and a warp runs its quartets in FP32 when every bound is below fp32_thr.
+  const double* Qp;   // Schwarz factor per pair
+  const float* dmax;  // [nshell * nshell] max |D| per shell block
+  int ns;
+  double skip_thr, fp32_thr;
 };
 
 struct SchwarzArgs {
@@ -58,11 +65,17 @@ struct EriClass;
 #define DSS_DEFINE_ERI_CLASS(la, lb, lc, ld, bc, kc)                                                    \
   template <>                                                                                           \
   struct EriClass<la, lb, lc, ld> {                                                                     \
+    template <int BOYS, bool PURE, typename R>                                                          \
+    __device__ __forceinline__ static void evalr(const PrimPair* bra, int nb, const PrimPair* ket, int nk, \
+                                                 double ABx, double ABy, double ABz, double CDx,        \
+                                                 double CDy, double CDz, R* I) {                        \
+      eri_##la##lb##lc##ld<BOYS, PURE, R>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I);          \
+    }                                                                                                   \
     template <int BOYS, bool PURE>                                                                      \
     __device__ __forceinline__ static void eval(const PrimPair* bra, int nb, const PrimPair* ket, int nk, \
                                                 double ABx, double ABy, double ABz, double CDx,         \
                                                 double CDy, double CDz, double* I) {                    \
-      eri_##la##lb##lc##ld<BOYS, PURE>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I);             \
+      eri_##la##lb##lc##ld<BOYS, PURE, double>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I);     \
     }                                                                                                   \
   };
 DSS_FOR_EACH_CLASS(DSS_DEFINE_ERI_CLASS)
@@ -74,7 +87,20 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-template <int LA, int LB, int LC, int LD, int BOYS, bool PURE>
+// Density bound of a quartet for the mixed-precision screen.
+__device__ __forceinline__ double quartet_dbound(const EriArgs& a, int sa, int sb, int sc, int sd) {
+  const float* dm = a.dmax;
+  const int ns = a.ns;
+  float m = dm[sc * ns + sd];
+  m = fmaxf(m, dm[sa * ns + sb]);
+  m = fmaxf(m, dm[sa * ns + sd]);
+  m = fmaxf(m, dm[sb * ns + sd]);
+  m = fmaxf(m, dm[sa * ns + sc]);
+  m = fmaxf(m, dm[sb * ns + sc]);
+  return (double)m;
+}
+
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false>
 __global__ void __launch_bounds__(128) eri_jk_kernel(EriArgs a) {
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
   constexpr int NC = dss_nfunc(LC, PURE), ND = dss_nfunc(LD, PURE);
@@ -82,18 +108,37 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(EriArgs a) {
   const int lane = threadIdx.x & 31;
   if (warp >= a.ntasks) return;  // uniform per warp
   const int4 t = __ldg(a.tasks + warp);
-  const bool active = lane < t.z;
+  bool active = lane < t.z;
   const int bra = t.x;
   const int ket = t.y + (active ? lane : 0);
   const int sa = __ldg(a.pair_a + bra), sb = __ldg(a.pair_b + bra);
   const int sc = __ldg(a.pair_a + ket), sd = __ldg(a.pair_b + ket);
+  bool fp32 = false;
+  if constexpr (MIXED) {
+    const double bound = __ldg(a.Qp + bra) * __ldg(a.Qp + ket) * quartet_dbound(a, sa, sb, sc, sd);
+    active = active && bound >= a.skip_thr;
+    fp32 = __all_sync(0xffffffffu, !active || bound < a.fp32_thr);
+  }
   const double Ax = __ldg(a.sh_xyz + 3 * sa), Ay = __ldg(a.sh_xyz + 3 * sa + 1), Az = __ldg(a.sh_xyz + 3 * sa + 2);
   const double Bx = __ldg(a.sh_xyz + 3 * sb), By = __ldg(a.sh_xyz + 3 * sb + 1), Bz = __ldg(a.sh_xyz + 3 * sb + 2);
   const double Cx = __ldg(a.sh_xyz + 3 * sc), Cy = __ldg(a.sh_xyz + 3 * sc + 1), Cz = __ldg(a.sh_xyz + 3 * sc + 2);
   const double Dx = __ldg(a.sh_xyz + 3 * sd), Dy = __ldg(a.sh_xyz + 3 * sd + 1), Dz = __ldg(a.sh_xyz + 3 * sd + 2);
 
   double I[NA * NB * NC * ND];
-  if (active) {
+  bool done = false;
+  if constexpr (MIXED) {
+    if (active && fp32) {
+      float If[NA * NB * NC * ND];
+      EriClass<LA, LB, LC, LD>::template evalr<BOYS, PURE, float>(
+          a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
+          __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, If);
+#pragma unroll
+      for (int q = 0; q < NA * NB * NC * ND; ++q) I[q] = (double)If[q];
+      done = true;
+    }
+  }
+  if (done) {
+  } else if (active) {
     EriClass<LA, LB, LC, LD>::template eval<BOYS, PURE>(
         a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
         __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, I);
@@ -221,13 +266,14 @@ __global__ void __launch_bounds__(128) schwarz_kernel(SchwarzArgs a) {
 
 // Host-side launchers (one translation unit per class defines them).
 #define DSS_DECLARE_LAUNCHERS(la, lb, lc, ld, bc, kc) \
-  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, const EriArgs& a, cudaStream_t s);
+  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, int mixed, const EriArgs& a, cudaStream_t s);
 DSS_FOR_EACH_CLASS(DSS_DECLARE_LAUNCHERS)
 #undef DSS_DECLARE_LAUNCHERS
 
 void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s);
 // variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class).
-void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant, const EriArgs& a,
-                            cudaStream_t s);
+void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int variant,
+                            const EriArgs& a, cudaStream_t s);
 bool dss_has_coop(int la, int lb, int lc, int ld);
-void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, const EriArgs& a, cudaStream_t s);
+void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, const EriArgs& a,
+                       cudaStream_t s);

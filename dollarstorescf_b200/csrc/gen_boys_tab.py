@@ -1,6 +1,6 @@
 """Generates boys_tab.cuh: F_m(x) on a grid for the fast (exact) Boys mode.
 
-Grid x_k = k / 16, k = 0..575 (x < 36), m = 0..15 (16 doubles per point, so the
+Grid x_k = k / 16, k = 0..575 (x < 36), m = 0..23 (24 doubles per point, so the
 seven Taylor coefficients F_{L..L+6}(x_k) a thread needs are contiguous and it
 fetches them with 16-byte loads).  Values come from
 F_m(x) = 1F1(m + 1/2; m + 3/2; -x) / (2m + 1) evaluated with mpmath at 40 digits.
@@ -12,7 +12,7 @@ import sys
 import mpmath
 
 NGRID = 576
-NM = 16
+NM = 24
 STEP = 16  # points per unit of x
 
 

@@ -173,9 +173,9 @@ class ClassGen:
             terms.append(f"WQ{ax} * {self.vrr(e, f1, m + 1)}")
             if f1[i] > 0:
                 f2 = sub1(f1, i)
-                terms.append(f"{lit(f1[i])} * oo2q * ({self.vrr(e, f2, m)} - rho_q * {self.vrr(e, f2, m + 1)})")
+                terms.append(f"(R){lit(f1[i])} * oo2q * ({self.vrr(e, f2, m)} - rho_q * {self.vrr(e, f2, m + 1)})")
             if e[i] > 0:
-                terms.append(f"{lit(e[i])} * oo2pq * {self.vrr(sub1(e, i), f1, m + 1)}")
+                terms.append(f"(R){lit(e[i])} * oo2pq * {self.vrr(sub1(e, i), f1, m + 1)}")
         else:
             i = pick_dir(e)
             e1 = sub1(e, i)
@@ -184,12 +184,12 @@ class ClassGen:
             terms.append(f"WP{ax} * {self.vrr(e1, f, m + 1)}")
             if e1[i] > 0:
                 e2 = sub1(e1, i)
-                terms.append(f"{lit(e1[i])} * oo2p * ({self.vrr(e2, f, m)} - rho_p * {self.vrr(e2, f, m + 1)})")
+                terms.append(f"(R){lit(e1[i])} * oo2p * ({self.vrr(e2, f, m)} - rho_p * {self.vrr(e2, f, m + 1)})")
         nterm = len(terms) + sum(1 for t in terms if "(" in t)  # bracketed terms carry two products
         self.flops_vrr += 2 * nterm
         if ne >= self.la and nf >= self.lc:
             self.flops_alg_vrr += 2 * nterm
-        self.vrr_lines.append(f"const double {name} = " + " + ".join(terms) + ";")
+        self.vrr_lines.append(f"const R {name} = " + " + ".join(terms) + ";")
         self.vrr_done[key] = name
         return name
 
@@ -207,22 +207,32 @@ class ClassGen:
         self.nacc = nE * nF
         o = out.append
         o(f"// ---- class ({la}{lb}|{lc}{ld}): L={L}, {nE}x{nF} contracted VRR outputs")
-        o(f"template <int BOYS, bool PURE>")
+        o(f"template <int BOYS, bool PURE, typename R = double>")
         o(f"__device__ __forceinline__ void eri_{self.name}(const PrimPair* __restrict__ bra, int nbra,")
-        o(f"    const PrimPair* __restrict__ ket, int nket, double ABx, double ABy, double ABz,")
-        o(f"    double CDx, double CDy, double CDz, double* __restrict__ I) {{")
-        o(f"  double acc[{nE * nF}];")
+        o(f"    const PrimPair* __restrict__ ket, int nket, double ABx_, double ABy_, double ABz_,")
+        o(f"    double CDx_, double CDy_, double CDz_, R* __restrict__ I) {{")
+        o(f"  const R ABx = (R)ABx_, ABy = (R)ABy_, ABz = (R)ABz_;")
+        o(f"  const R CDx = (R)CDx_, CDy = (R)CDy_, CDz = (R)CDz_;")
+        o(f"  R acc[{nE * nF}];")
         o(f"#pragma unroll")
-        o(f"  for (int t = 0; t < {nE * nF}; ++t) acc[t] = 0.0;")
+        o(f"  for (int t = 0; t < {nE * nF}; ++t) acc[t] = (R)0.0;")
         o(f"  for (int ik = 0; ik < nket; ++ik) {{")
         o(f"    const PrimPair kp = load_pp(ket + ik);")
         o(f"    for (int ib = 0; ib < nbra; ++ib) {{")
         o(f"      const PrimPair bp = load_pp(bra + ib);")
-        o(f"      double F[{L + 1}];")
-        o(f"      double PAx, PAy, PAz, WPx, WPy, WPz, QCx, QCy, QCz, WQx, WQy, WQz;")
-        o(f"      double oo2p, oo2q, oo2pq, rho_p, rho_q;")
-        o(f"      prim_quartet<BOYS, {L}>(bp, kp, F, PAx, PAy, PAz, WPx, WPy, WPz, QCx, QCy, QCz, WQx, WQy, WQz,")
-        o(f"                              oo2p, oo2q, oo2pq, rho_p, rho_q);")
+        o(f"      double Fd[{L + 1}];")
+        o(f"      double PAx_, PAy_, PAz_, WPx_, WPy_, WPz_, QCx_, QCy_, QCz_, WQx_, WQy_, WQz_;")
+        o(f"      double oo2p_, oo2q_, oo2pq_, rho_p_, rho_q_;")
+        o(f"      prim_quartet<BOYS, {L}>(bp, kp, Fd, PAx_, PAy_, PAz_, WPx_, WPy_, WPz_, QCx_, QCy_, QCz_, WQx_,")
+        o(f"                              WQy_, WQz_, oo2p_, oo2q_, oo2pq_, rho_p_, rho_q_);")
+        o(f"      R F[{L + 1}];")
+        o(f"#pragma unroll")
+        o(f"      for (int m = 0; m <= {L}; ++m) F[m] = (R)Fd[m];")
+        o(f"      const R PAx = (R)PAx_, PAy = (R)PAy_, PAz = (R)PAz_, WPx = (R)WPx_, WPy = (R)WPy_, WPz = (R)WPz_;")
+        o(f"      const R QCx = (R)QCx_, QCy = (R)QCy_, QCz = (R)QCz_, WQx = (R)WQx_, WQy = (R)WQy_, WQz = (R)WQz_;")
+        o(f"      const R oo2p = (R)oo2p_, oo2q = (R)oo2q_, oo2pq = (R)oo2pq_, rho_p = (R)rho_p_, rho_q = (R)rho_q_;")
+        o(f"      (void)PAx; (void)PAy; (void)PAz; (void)WPx; (void)WPy; (void)WPz; (void)QCx; (void)QCy; (void)QCz;")
+        o(f"      (void)WQx; (void)WQy; (void)WQz; (void)oo2p; (void)oo2q; (void)oo2pq; (void)rho_p; (void)rho_q;")
         for line in self.vrr_lines:
             o("      " + line)
         for e in ecomps:
@@ -248,7 +258,7 @@ class ClassGen:
             x = hbra(add1(a, i), b1, fi)
             y = hbra(a, b1, fi)
             nm = f"hb{cname(a)}_{cname(b)}_{fi}"
-            hlines.append(f"const double {nm} = {x} + AB{'xyz'[i]} * {y};")
+            hlines.append(f"const R {nm} = {x} + AB{'xyz'[i]} * {y};")
             self.flops_hrr += 2
             hb[key] = nm
             return nm
@@ -271,7 +281,7 @@ class ClassGen:
             x = hket(a, b, add1(c, i), d1)
             y = hket(a, b, c, d1)
             nm = f"hk{cname(a)}_{cname(b)}_{cname(c)}_{cname(d)}"
-            hlines.append(f"const double {nm} = {x} + CD{'xyz'[i]} * {y};")
+            hlines.append(f"const R {nm} = {x} + CD{'xyz'[i]} * {y};")
             self.flops_hrr += 2
             hk[key] = nm
             return nm
@@ -306,7 +316,7 @@ class ClassGen:
                     if len(terms) == 1 and terms[0][0] == 1.0:
                         new[idx] = terms[0][1]
                         continue
-                    o(f"    const double {nm} = " + " + ".join(f"{lit(w)} * {s}" for w, s in terms) + ";")
+                    o(f"    const R {nm} = " + " + ".join(f"(R){lit(w)} * {s}" for w, s in terms) + ";")
                     new[idx] = nm
                 cur = new
                 dims = newdims

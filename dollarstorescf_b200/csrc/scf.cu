@@ -232,6 +232,11 @@ void dss_default_scf_opts(dss_scf_opts* o) {
   o->diis_size = 8;  // diis::setIterationCount(8), SCFSolver.cpp:214
   o->max_iter = 128;
   o->use_guess = 0;
+  o->incremental = 0;
+  o->fp32_threshold = 1e-7;
+  o->skip_threshold = 1e-12;
+  o->rebuild_every = 8;
+  o->final_switch = 1e-5;
 }
 
 int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha, double e_nuc,
@@ -254,13 +259,15 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
   // Device buffers (kept in the context so repeated solves reuse them).
   ScfBuffers& b = ctx->scf;
   const int ds = o.diis_size;
-  const size_t need = n2 * (14 + 2 * (size_t)ds) + 3 * n2 + 8 * (size_t)n + 256;
+  const size_t need = n2 * (16 + 2 * (size_t)ds) + 3 * n2 + 8 * (size_t)n + 256;
   if (b.pool.resize(need) != cudaSuccess || b.ibuf.resize(8 + 2 * (size_t)n) != cudaSuccess)
     return dss_fail(ctx, DSS_ERR_OOM, "dss_scf_solve: device allocation failed");
   double* base = b.pool.ptr;
   double *H = base, *S = H + n2, *X = S + n2, *D = X + n2, *Dt = D + n2, *J = Dt + n2, *K = J + n2, *G = K + n2,
          *F = G + n2, *Fn = F + n2, *T1 = Fn + n2, *T2 = T1 + n2, *Cp = T2 + n2, *C = Cp + n2;
-  double* Fring = C + n2;
+  double* Gprev = C + n2;  // incremental form: G and D of the previous build
+  double* Dprev = Gprev + n2;
+  double* Fring = Dprev + n2;
   double* Ering = Fring + (size_t)ds * n2;
   double* work = Ering + (size_t)ds * n2;           // 3 n^2 + 64 + n ints
   double* eps = work + 3 * n2 + 64 + (size_t)n;    // n
@@ -301,19 +308,54 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
   double E = 0.0, E_prev = 0.0;
   int it = 0;
   int rc = DSS_OK;
+  // Full builds: the plain form always; the incremental form at the start, every
+  // rebuild_every iterations and throughout the final phase.
+  BuildMode full_mode;
+  full_mode.boys = o.incremental ? DSS_BOYS_FAST : ctx->opts.boys_mode;
+  int last_full = -1000, full_streak = 0;
+  bool final_phase = !o.incremental;
+  if (o.incremental) {
+    if (ctx->d_dmax.resize((size_t)ctx->nshell * ctx->nshell) != cudaSuccess)
+      return dss_fail(ctx, DSS_ERR_OOM, "dss_scf_solve: device allocation failed");
+  }
   while (true) {
-    if (it && std::fabs(E - E_prev) < o.conv) break;
+    if (it && std::fabs(E - E_prev) < o.conv && full_streak >= (o.incremental ? 2 : 0)) break;
+    if (o.incremental && it && std::fabs(E - E_prev) < o.final_switch) final_phase = true;
     if (it >= o.max_iter) {
       rc = dss_fail(ctx, DSS_ERR_NOCONV, "dss_scf_solve: no convergence within max_iter iterations");
       break;
     }
     ++it;
-    // G = J[2D] - K[2D]/2
-    axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 2.0, D, 0.0, D, 0.0, nullptr, Dt);
-    int r2 = dss_enqueue_jk(ctx, Dt, J, K);
-    if (r2 != DSS_OK) return r2;
-    // J, K hold the accumulators: G = (J + J^T) - (K + K^T)/2
-    dss_symmetrize_combine(s, n, J, K, G);
+    const bool full = !o.incremental || final_phase || it <= 2 || it - last_full >= o.rebuild_every;
+    if (full) {
+      // G = J[2D] - K[2D]/2
+      axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 2.0, D, 0.0, D, 0.0, nullptr, Dt);
+      int r2 = dss_enqueue_jk(ctx, Dt, J, K, nullptr, &full_mode);
+      if (r2 != DSS_OK) return r2;
+      // J, K hold the accumulators: G = (J + J^T) - (K + K^T)/2
+      dss_symmetrize_combine(s, n, J, K, G);
+      last_full = it;
+      ++full_streak;
+    } else {
+      // G = G_prev + G[2 (D - D_prev)] with the screened mixed-precision kernels.
+      axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 2.0, D, -2.0, Dprev, 0.0, nullptr, Dt);
+      dss_block_max(ctx, Dt, ctx->d_dmax.ptr);
+      BuildMode mm;
+      mm.boys = DSS_BOYS_FAST;
+      mm.mixed = 1;
+      mm.dmax = ctx->d_dmax.ptr;
+      mm.fp32_thr = o.fp32_threshold;
+      mm.skip_thr = o.skip_threshold;
+      int r2 = dss_enqueue_jk(ctx, Dt, J, K, nullptr, &mm);
+      if (r2 != DSS_OK) return r2;
+      dss_symmetrize_combine(s, n, J, K, T1);
+      axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 1.0, Gprev, 1.0, T1, 0.0, nullptr, G);
+      full_streak = 0;
+    }
+    if (o.incremental) {
+      SCF_CHECK(cudaMemcpyAsync(Gprev, G, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy G");
+      SCF_CHECK(cudaMemcpyAsync(Dprev, D, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy D");
+    }
     axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 1.0, H, 1.0, G, 0.0, nullptr, Fn);
     if (it == 1) {
       SCF_CHECK(cudaMemcpyAsync(F, Fn, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy F");
@@ -360,9 +402,9 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
       break;
     }
   }
-  // Final energy from the final density (calculateEnergies).
+  // Final energy from the final density (calculateEnergies), FP64.
   axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 2.0, D, 0.0, D, 0.0, nullptr, Dt);
-  int r3 = dss_enqueue_jk(ctx, Dt, J, K);
+  int r3 = dss_enqueue_jk(ctx, Dt, J, K, nullptr, &full_mode);
   if (r3 != DSS_OK) return r3;
   dss_symmetrize_combine(s, n, J, K, G);
   SCF_CHECK(cudaMemsetAsync(small + 1, 0, 16, s), "zero tr");

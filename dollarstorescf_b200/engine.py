@@ -100,6 +100,11 @@ class FockBuilder:
                                          ctypes.cast(J_ptr, ctypes.POINTER(ctypes.c_double)),
                                          ctypes.cast(K_ptr, ctypes.POINTER(ctypes.c_double))))
 
+    def jk_mixed_device(self, D_ptr: int, J_ptr: int, K_ptr: int, fp32_threshold: float = 1e-7,
+                        skip_threshold: float = 1e-12) -> None:
+        self._check(self._L.dss_build_jk_mixed_device(self._h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(J_ptr),
+                                                      ctypes.c_void_p(K_ptr), fp32_threshold, skip_threshold))
+
     def stream_ptr(self) -> int:
         return int(self._L.dss_get_stream(self._h) or 0)
 
@@ -156,10 +161,13 @@ class FockBuilder:
 
     def scf(self, H: np.ndarray, S: np.ndarray, n_alpha: int, e_nuc: float, conv: float = 1e-8,
             diis_size: int = 8, max_iter: int = 128, guess: Optional[np.ndarray] = None,
-            raise_on_noconv: bool = True):
-        """Device RHF.  Returns (E_total, D_alpha packed-U, iterations, status)."""
+            raise_on_noconv: bool = True, mixed: bool = False, fp32_threshold: float = 1e-7,
+            skip_threshold: float = 1e-12, rebuild_every: int = 8, final_switch: float = 1e-5):
+        """Device RHF.  Returns (E_total, D_alpha packed-U, iterations, status).
+        mixed=True selects the incremental mixed-precision form."""
         n = self.nbf
-        o = _lib.DssScfOpts(conv, diis_size, max_iter, 1 if guess is not None else 0)
+        o = _lib.DssScfOpts(conv, diis_size, max_iter, 1 if guess is not None else 0, 1 if mixed else 0,
+                            fp32_threshold, skip_threshold, rebuild_every, final_switch)
         D = np.ascontiguousarray(guess, dtype=np.float64).copy() if guess is not None else np.zeros(n * (n + 1) // 2)
         E = ctypes.c_double()
         it = ctypes.c_int()

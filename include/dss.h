@@ -79,6 +79,15 @@ int dss_build_jk(dss_ctx* ctx, const double* D_packed, double* J_packed, double*
  * synchronises with dss_sync().  For callers that keep densities in HBM. */
 int dss_build_jk_device(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev);
 
+/* Mixed-precision, density-screened build (the incremental form's kernel):
+ * quartets whose bound Q_ab Q_cd max|D| (over the six density blocks they
+ * touch) is below skip_threshold are skipped; a warp of quartets whose bounds
+ * are all below fp32_threshold runs the recurrences in FP32.  The Boys
+ * function, the Schwarz factors and all accumulation stay FP64; the Boys
+ * function is the accurate one.  Device-resident dense matrices as above. */
+int dss_build_jk_mixed_device(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev,
+                              double fp32_threshold, double skip_threshold);
+
 /* Waits for the context's stream. */
 int dss_sync(dss_ctx* ctx);
 
@@ -143,10 +152,21 @@ typedef struct dss_scf_opts {
   int diis_size; /* Pulay DIIS ring length, 1..9 */
   int max_iter;  /* iteration cap (the reference loops until converged) */
   int use_guess; /* 0: core guess D = 0 (scf::useCoreGuess); 1: start from D_alpha_inout */
+  /* Mixed-precision incremental form (incremental = 1): G(D_k) = G(D_k-1) +
+   * G(D_k - D_k-1), each increment built by dss_build_jk_mixed_device with the
+   * thresholds below; a full FP64 build every rebuild_every iterations and for
+   * every iteration once |dE| < final_switch (so the last two iterations and the
+   * energy are FP64).  incremental = 0 is the plain form: a full FP64 build with
+   * the context's Boys mode every iteration. */
+  int incremental;
+  double fp32_threshold; /* default 1e-7 */
+  double skip_threshold; /* default 1e-12 */
+  int rebuild_every;     /* default 8 */
+  double final_switch;   /* default 1e-5 Eh */
 } dss_scf_opts;
 
 /* Defaults: conv 1e-8 (chem/scf/SCFSolver.cpp:26), diis_size 8 (:214),
- * max_iter 128, core guess. */
+ * max_iter 128, core guess, plain form. */
 void dss_default_scf_opts(dss_scf_opts* opts);
 
 /* Closed-shell RHF on the device for the current basis, replacing
