@@ -31,7 +31,8 @@ class DssScfOpts(ctypes.Structure):
 
 
 class DssOpts(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int), ("schwarz_threshold", ctypes.c_double), ("boys_mode", ctypes.c_int)]
+    _fields_ = [("device", ctypes.c_int), ("schwarz_threshold", ctypes.c_double), ("boys_mode", ctypes.c_int),
+                ("primitive_threshold", ctypes.c_double)]
 
 
 def header_symbols():
@@ -102,5 +103,29 @@ def load():
     L.dss_scf_solve.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(DssScfOpts), dp, dp,
                                 ip]
     L.dss_scf_solve.restype = ctypes.c_int
+    szt = ctypes.c_size_t
+    L.dss_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(DssOpts), szt, ctypes.c_int]
+    L.dss_batch_create.restype = ctypes.c_int
+    L.dss_batch_destroy.argtypes = [vp]
+    L.dss_batch_destroy.restype = None
+    L.dss_batch_last_error.argtypes = [vp]
+    L.dss_batch_last_error.restype = ctypes.c_char_p
+    L.dss_batch_add.argtypes = [vp, ctypes.c_int, ip, ip, dp, dp, dp, ctypes.c_int, ctypes.c_int, ip, dp,
+                                ctypes.c_int, dp, ip]
+    L.dss_batch_add.restype = ctypes.c_int
+    L.dss_batch_step.argtypes = [vp, ctypes.POINTER(DssScfOpts), ctypes.c_int, ip]
+    L.dss_batch_step.restype = ctypes.c_int
+    L.dss_batch_solve.argtypes = [vp, ctypes.POINTER(DssScfOpts)]
+    L.dss_batch_solve.restype = ctypes.c_int
+    L.dss_batch_result.argtypes = [vp, ctypes.c_int, dp, dp, ip, ip]
+    L.dss_batch_result.restype = ctypes.c_int
+    L.dss_batch_remove.argtypes = [vp, ctypes.c_int]
+    L.dss_batch_remove.restype = ctypes.c_int
+    L.dss_batch_info.argtypes = [vp, ip, llp, llp]
+    L.dss_batch_info.restype = ctypes.c_int
+    L.dss_batch_set_class_variant.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.dss_batch_set_class_variant.restype = ctypes.c_int
+    L.dss_batch_context.argtypes = [vp]
+    L.dss_batch_context.restype = vp
     _lib = L
     return L

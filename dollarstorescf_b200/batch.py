@@ -1,0 +1,101 @@
+"""Python mirror of the batch C ABI (dss_batch_*): many molecules solved
+together, with molecules joining and leaving between SCF iterations."""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from .engine import BOYS_REF, _dp, _ip
+from .shells import ShellArrays
+
+
+class Batch:
+    def __init__(self, device: int = 0, schwarz_threshold: float = 1e-12, boys_mode: int = BOYS_REF,
+                 arena_bytes: int = 0, diis_size: int = 8, primitive_threshold: float = 1e-18):
+        self._L = _lib.load()
+        opts = _lib.DssOpts(device, schwarz_threshold, boys_mode, primitive_threshold)
+        h = ctypes.c_void_p()
+        rc = self._L.dss_batch_create(ctypes.byref(h), ctypes.byref(opts), arena_bytes, diis_size)
+        if rc != 0:
+            raise _lib.DssError(rc, self._L.dss_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise _lib.DssError(rc, self._L.dss_batch_last_error(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.dss_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, sh: ShellArrays, charge: int = 0, guess: Optional[np.ndarray] = None) -> int:
+        """Admits a molecule; raises DssError with code -2 when the arena is full."""
+        l = np.ascontiguousarray(sh.shell_l, dtype=np.int32)
+        n = np.ascontiguousarray(sh.shell_nprim, dtype=np.int32)
+        e = np.ascontiguousarray(sh.exps, dtype=np.float64)
+        c = np.ascontiguousarray(sh.coefs, dtype=np.float64)
+        x = np.ascontiguousarray(sh.centers, dtype=np.float64).ravel()
+        Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
+        ax = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
+        g = np.ascontiguousarray(guess, dtype=np.float64) if guess is not None else None
+        h = ctypes.c_int()
+        self._check(self._L.dss_batch_add(self._h, sh.nshell, _ip(l), _ip(n), _dp(e), _dp(c), _dp(x),
+                                          1 if sh.pure else 0, sh.natom, _ip(Z), _dp(ax), charge,
+                                          _dp(g) if g is not None else None, ctypes.byref(h)))
+        return h.value
+
+    @staticmethod
+    def opts(conv: float = 1e-8, diis_size: int = 8, max_iter: int = 128):
+        return _lib.DssScfOpts(conv, diis_size, max_iter, 0, 0, 1e-7, 1e-12, 8, 1e-5)
+
+    def step(self, iterations: int = 1, conv: float = 1e-8, max_iter: int = 128) -> int:
+        o = self.opts(conv, max_iter=max_iter)
+        act = ctypes.c_int()
+        self._check(self._L.dss_batch_step(self._h, ctypes.byref(o), iterations, ctypes.byref(act)))
+        return act.value
+
+    def solve(self, conv: float = 1e-8, max_iter: int = 128) -> None:
+        o = self.opts(conv, max_iter=max_iter)
+        self._check(self._L.dss_batch_solve(self._h, ctypes.byref(o)))
+
+    def result(self, handle: int, nbf: int = 0, want_density: bool = False) -> Tuple[float, Optional[np.ndarray], int, int]:
+        E = ctypes.c_double()
+        it = ctypes.c_int()
+        st = ctypes.c_int()
+        D = np.empty(nbf * (nbf + 1) // 2) if want_density else None
+        self._check(self._L.dss_batch_result(self._h, handle, ctypes.byref(E), _dp(D) if D is not None else None,
+                                             ctypes.byref(it), ctypes.byref(st)))
+        return E.value, D, it.value, st.value
+
+    def finished(self, handle: int) -> bool:
+        E = ctypes.c_double()
+        return self._L.dss_batch_result(self._h, handle, ctypes.byref(E), None, None, None) == 0
+
+    def remove(self, handle: int) -> None:
+        self._check(self._L.dss_batch_remove(self._h, handle))
+
+    def info(self, n_for_region: int = 0) -> Tuple[int, int, int]:
+        nl = ctypes.c_int()
+        fb = ctypes.c_longlong()
+        rb = ctypes.c_longlong(n_for_region)
+        self._check(self._L.dss_batch_info(self._h, ctypes.byref(nl), ctypes.byref(fb), ctypes.byref(rb)))
+        return nl.value, fb.value, rb.value if n_for_region else 0
+
+    def set_class_variant(self, i: int, variant: int) -> None:
+        self._check(self._L.dss_batch_set_class_variant(self._h, i, variant))

@@ -1,0 +1,1045 @@
+// Batched RHF: many molecules of uneven size in one set of launches.
+//
+// Every admitted molecule owns one region of a device arena: a small header
+// (energies, iteration counter, DIIS state) followed by its n x n matrices and
+// DIIS rings.  Regions stay in place while their molecule is in the batch, so
+// molecules can join and leave between iterations (the serving loop's
+// continuous batching) without moving the others.  Admission is by arena space.
+//
+// The batch's shells form one basis whose shell pairs and work lists never mix
+// molecules (dss_setup_pairs with per-shell molecule ids); each ERI class is one
+// launch over all molecules, reading and writing every molecule's own matrices
+// through per-shell offsets.  The SCF steps run as batched kernels (one grid
+// dimension over molecules): the reference's iteration (chem/scf/SCFSolver.cpp:
+// 145-177: G, F, Pulay DIIS, X F X, eigenvectors, density, energy, convergence)
+// with all per-molecule control (iteration count, DIIS ring, convergence flag)
+// on the device, so one captured CUDA graph replays the same iteration for
+// every molecule whatever its stage.  The eigensolver is the cyclic Jacobi
+// method with one thread block per molecule, the matrix held in shared memory
+// when it fits, warm-started from the previous iteration's vectors.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dss.h"
+#include "dss_internal.h"
+#include "linalg.cuh"
+
+namespace {
+
+// Region layout (doubles): header, then matrices of n*n each, then rings, eps.
+constexpr int kHdr = 256;
+enum Mat { M_H, M_S, M_X, M_D, M_DT, M_J, M_K, M_G, M_FN, M_F, M_T1, M_T2, M_CP, M_C, M_V, M_T3, M_NMAT };
+// Header slots
+constexpr int H_E = 0, H_EPREV = 1, H_TRDG = 2, H_ENUC = 3, H_DOTS = 4, H_COEF = 16, H_B = 32, H_TRDH = 140,
+              H_EFINAL = 141, H_INT = 200;
+// Integer header (as int view of doubles from H_INT): iteration, done, diis count, diis slot, nocc, n, status
+constexpr int I_IT = 0, I_DONE = 1, I_CNT = 2, I_SLOT = 3, I_NOCC = 4, I_N = 5, I_STATUS = 6, I_FINAL = 7;
+
+__host__ __device__ inline size_t region_size(int n, int ds) {
+  const size_t n2 = (size_t)n * n;
+  size_t s = kHdr + (size_t)M_NMAT * n2 + 2 * (size_t)ds * n2 + (size_t)n + 8;
+  return (s + 31) & ~(size_t)31;  // 256-byte granules
+}
+__device__ __forceinline__ double* mat(double* base, int n, int k) { return base + kHdr + (size_t)k * n * n; }
+__device__ __forceinline__ double* ring_f(double* base, int n, int ds, int slot) {
+  return base + kHdr + (size_t)M_NMAT * n * n + (size_t)slot * n * n;
+}
+__device__ __forceinline__ double* ring_e(double* base, int n, int ds, int slot) {
+  return base + kHdr + (size_t)(M_NMAT + ds) * n * n + (size_t)slot * n * n;
+}
+__device__ __forceinline__ double* eps_of(double* base, int n, int ds) {
+  return base + kHdr + (size_t)(M_NMAT + 2 * ds) * n * n;
+}
+__device__ __forceinline__ int* ihdr(double* base) { return reinterpret_cast<int*>(base + H_INT); }
+
+struct BatchView {
+  double* arena;
+  const long long* region;  // per batch slot
+  const int* nvec;
+  const int* active;        // per batch slot
+  int nb, ds;
+};
+
+#define BV_BEGIN()                                   \
+  const int b = blockIdx.y;                          \
+  if (b >= v.nb || !v.active[b]) return;             \
+  const int n = v.nvec[b];                           \
+  double* base = v.arena + v.region[b];              \
+  const long long n2 = (long long)n * n;             \
+  (void)n2;
+
+// Dt = 2 D, J = K = 0
+__global__ void k_prep(BatchView v) {
+  BV_BEGIN();
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    mat(base, n, M_DT)[t] = 2.0 * mat(base, n, M_D)[t];
+    mat(base, n, M_J)[t] = 0.0;
+    mat(base, n, M_K)[t] = 0.0;
+  }
+}
+
+// G = (J + J^T) - (K + K^T)/2, F_new = H + G
+__global__ void k_fock(BatchView v) {
+  BV_BEGIN();
+  const double* J = mat(base, n, M_J);
+  const double* K = mat(base, n, M_K);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    const long long u = (long long)c * n + r;
+    const double g = (J[t] + J[u]) - 0.5 * (K[t] + K[u]);
+    mat(base, n, M_G)[t] = g;
+    mat(base, n, M_FN)[t] = mat(base, n, M_H)[t] + g;
+  }
+}
+
+// C = alpha op(A) op(B) + beta C per molecule (matrix indices into the region).
+__global__ void k_gemm(BatchView v, int ka, int kb, int kc, int ta, int tb, double alpha, double beta) {
+  const int b = blockIdx.z;
+  if (b >= v.nb || !v.active[b]) return;
+  const int n = v.nvec[b];
+  const int row0 = blockIdx.y * 32, col0 = blockIdx.x * 32;
+  if (row0 >= n || col0 >= n) return;
+  double* base = v.arena + v.region[b];
+  const double* A = mat(base, n, ka);
+  const double* B = mat(base, n, kb);
+  double* C = mat(base, n, kc);
+  __shared__ double As[32][33];
+  __shared__ double Bs[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < n; k0 += 32) {
+    for (int r = ty; r < 32; r += 8) {
+      const int i = row0 + r, k = k0 + tx;
+      As[r][tx] = (i < n && k < n) ? (ta ? A[(size_t)k * n + i] : A[(size_t)i * n + k]) : 0.0;
+      const int kk = k0 + r, j = col0 + tx;
+      Bs[r][tx] = (kk < n && j < n) ? (tb ? B[(size_t)j * n + kk] : B[(size_t)kk * n + j]) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const double bv = Bs[k][tx];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] += As[ty + 8 * q][k] * bv;
+    }
+    __syncthreads();
+  }
+  for (int q = 0; q < 4; ++q) {
+    const int i = row0 + ty + 8 * q, j = col0 + tx;
+    if (i < n && j < n) {
+      const size_t o = (size_t)i * n + j;
+      C[o] = alpha * acc[q] + (beta == 0.0 ? 0.0 : beta * C[o]);
+    }
+  }
+}
+
+// DIIS slot choice (lalib/DIIS.ipp:19-62) for molecules in their second or later iteration.
+__global__ void k_diis_choose(BatchView v) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb || !v.active[b]) return;
+  double* base = v.arena + v.region[b];
+  int* ih = ihdr(base);
+  for (int i = 0; i < 10; ++i) base[H_DOTS + i] = 0.0;
+  if (ih[I_IT] < 1) return;  // first iteration: F = F_new
+  int count = ih[I_CNT], slot = 0;
+  if (count < v.ds) {
+    slot = count;
+    ++count;
+  } else {
+    double mx = 0.0;
+    for (int i = 0; i < v.ds; ++i) {
+      const double e = base[H_B + i * 10 + i];
+      if (e > mx) {
+        mx = e;
+        slot = i;
+      }
+    }
+  }
+  ih[I_CNT] = count;
+  ih[I_SLOT] = slot;
+}
+
+// e = T2 - T2^T and F_new into the chosen ring slots.
+__global__ void k_diis_store(BatchView v) {
+  BV_BEGIN();
+  int* ih = ihdr(base);
+  if (ih[I_IT] < 1) return;
+  const int slot = ih[I_SLOT];
+  const double* T2 = mat(base, n, M_T2);
+  double* e = ring_e(base, n, v.ds, slot);
+  double* f = ring_f(base, n, v.ds, slot);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    e[t] = T2[t] - T2[(long long)c * n + r];
+    f[t] = mat(base, n, M_FN)[t];
+  }
+}
+
+// dots[i] = <e_i, e_slot>; blockIdx.z = ring entry.
+__global__ void k_diis_dots(BatchView v) {
+  BV_BEGIN();
+  int* ih = ihdr(base);
+  const int i = blockIdx.z;
+  if (ih[I_IT] < 1 || i >= ih[I_CNT]) return;
+  const double* a = ring_e(base, n, v.ds, i);
+  const double* c = ring_e(base, n, v.ds, ih[I_SLOT]);
+  double acc = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+    acc += a[t] * c[t];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+    atomicAdd(base + H_DOTS + i, s);
+  }
+}
+
+// Bordered B c = (0,..,0,1) by Gaussian elimination with partial pivoting; a
+// singular system keeps only the newest Fock matrix.
+__global__ void k_diis_solve(BatchView v) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb || !v.active[b]) return;
+  double* base = v.arena + v.region[b];
+  int* ih = ihdr(base);
+  if (ih[I_IT] < 1) return;
+  const int count = ih[I_CNT], slot = ih[I_SLOT];
+  double* B = base + H_B;
+  double* coef = base + H_COEF;
+  for (int i = 0; i < count; ++i) {
+    B[slot * 10 + i] = base[H_DOTS + i];
+    B[i * 10 + slot] = base[H_DOTS + i];
+  }
+  const int m = count + 1;
+  double M[10][11];
+  for (int i = 0; i < m; ++i) {
+    for (int j = 0; j < m; ++j) M[i][j] = (i < count && j < count) ? B[i * 10 + j] : ((i == count && j == count) ? 0.0 : 1.0);
+    M[i][m] = (i == count) ? 1.0 : 0.0;
+  }
+  bool singular = false;
+  for (int k = 0; k < m; ++k) {
+    int piv = k;
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(M[i][k]) > fabs(M[piv][k])) piv = i;
+    if (M[piv][k] == 0.0) {
+      singular = true;
+      break;
+    }
+    if (piv != k)
+      for (int j = 0; j <= m; ++j) {
+        const double t = M[k][j];
+        M[k][j] = M[piv][j];
+        M[piv][j] = t;
+      }
+    for (int i = k + 1; i < m; ++i) {
+      const double f = M[i][k] / M[k][k];
+      for (int j = k; j <= m; ++j) M[i][j] -= f * M[k][j];
+    }
+  }
+  if (!singular) {
+    double x[10];
+    for (int i = m - 1; i >= 0; --i) {
+      double s = M[i][m];
+      for (int j = i + 1; j < m; ++j) s -= M[i][j] * x[j];
+      x[i] = s / M[i][i];
+    }
+    for (int i = 0; i < count; ++i) coef[i] = x[i];
+  } else {
+    for (int i = 0; i < count; ++i) coef[i] = (i == slot) ? 1.0 : 0.0;
+  }
+}
+
+// F = sum_i c_i F_i (iteration >= 2) or F = F_new (first iteration)
+__global__ void k_diis_combine(BatchView v) {
+  BV_BEGIN();
+  int* ih = ihdr(base);
+  const int count = ih[I_CNT];
+  const bool first = ih[I_IT] < 1;
+  double* F = mat(base, n, M_F);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    if (first) {
+      F[t] = mat(base, n, M_FN)[t];
+    } else {
+      double s = 0.0;
+      for (int i = 0; i < count; ++i) s += base[H_COEF + i] * ring_f(base, n, v.ds, i)[t];
+      F[t] = s;
+    }
+  }
+}
+
+__device__ __forceinline__ void rr_pair(int m, int r, int k, int& p, int& q) {
+  if (k == 0) {
+    p = m - 1;
+    q = r;
+  } else {
+    p = (r + k) % (m - 1);
+    q = (r - k + (m - 1)) % (m - 1);
+  }
+  if (p > q) {
+    const int t = p;
+    p = q;
+    q = t;
+  }
+}
+
+// Cyclic Jacobi, one block per molecule: A (matrix ka, overwritten) -> eigenvalues
+// ascending in eps, eigenvectors as columns of matrix kv (via the spare kt).
+template <bool SMEM>
+__global__ void __launch_bounds__(256) k_jacobi(BatchView v, int ka, int kv, int kt, int max_sweeps, double tol) {
+  const int b = blockIdx.x;
+  if (b >= v.nb || !v.active[b]) return;
+  const int n = v.nvec[b];
+  double* base = v.arena + v.region[b];
+  extern __shared__ double sm[];
+  const int m = (n % 2) ? n + 1 : n;
+  const int half = m / 2;
+  double* A = SMEM ? sm : mat(base, n, ka);
+  double* cs = SMEM ? sm + (size_t)n * n : sm;
+  double* V = mat(base, n, kv);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (SMEM)
+    for (int t = tid; t < n * n; t += nt) A[t] = mat(base, n, ka)[t];
+  for (int t = tid; t < n * n; t += nt) V[t] = (t / n == t % n) ? 1.0 : 0.0;
+  __shared__ double red[2][8];
+  __syncthreads();
+  for (int sweep = 0; sweep <= max_sweeps; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int t = tid; t < n * n; t += nt) {
+      const double x = A[t];
+      if (t / n == t % n) dia += x * x;
+      else off += x * x;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      dia += __shfl_xor_sync(0xffffffffu, dia, o);
+    }
+    if ((tid & 31) == 0) {
+      red[0][tid >> 5] = off;
+      red[1][tid >> 5] = dia;
+    }
+    __syncthreads();
+    double so = 0.0, sd = 0.0;
+    for (int k = 0; k < (nt >> 5); ++k) {
+      so += red[0][k];
+      sd += red[1][k];
+    }
+    __syncthreads();
+    if (so <= tol * tol * (so + sd) || sweep == max_sweeps) break;
+    for (int r = 0; r < m - 1; ++r) {
+      for (int k = tid; k < half; k += nt) {
+        int p, q;
+        rr_pair(m, r, k, p, q);
+        double c = 1.0, s = 0.0;
+        if (q < n) {
+          const double apq = A[p * n + q];
+          if (fabs(apq) > 1e-300) {
+            const double app = A[p * n + p], aqq = A[q * n + q];
+            const double tau = (aqq - app) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        cs[k] = c;
+        cs[half + k] = s;
+      }
+      __syncthreads();
+      for (int t = tid; t < half * half; t += nt) {
+        const int k1 = t / half, k2 = t % half;
+        int p1, q1, p2, q2;
+        rr_pair(m, r, k1, p1, q1);
+        rr_pair(m, r, k2, p2, q2);
+        const double c1 = cs[k1], s1 = cs[half + k1], c2 = cs[k2], s2 = cs[half + k2];
+        const bool q1v = q1 < n, q2v = q2 < n;
+        const double b00 = A[p1 * n + p2];
+        const double b01 = q2v ? A[p1 * n + q2] : 0.0;
+        const double b10 = q1v ? A[q1 * n + p2] : 0.0;
+        const double b11 = (q1v && q2v) ? A[q1 * n + q2] : 0.0;
+        const double x00 = c1 * b00 - s1 * b10, x01 = c1 * b01 - s1 * b11;
+        const double x10 = s1 * b00 + c1 * b10, x11 = s1 * b01 + c1 * b11;
+        A[p1 * n + p2] = x00 * c2 - x01 * s2;
+        if (q2v) A[p1 * n + q2] = x00 * s2 + x01 * c2;
+        if (q1v) A[q1 * n + p2] = x10 * c2 - x11 * s2;
+        if (q1v && q2v) A[q1 * n + q2] = x10 * s2 + x11 * c2;
+      }
+      for (int t = tid; t < n * half; t += nt) {
+        const int i = t / half, k = t % half;
+        int p, q;
+        rr_pair(m, r, k, p, q);
+        if (q >= n) continue;
+        const double c = cs[k], s = cs[half + k];
+        const double vp = V[(size_t)i * n + p], vq = V[(size_t)i * n + q];
+        V[(size_t)i * n + p] = c * vp - s * vq;
+        V[(size_t)i * n + q] = s * vp + c * vq;
+      }
+      __syncthreads();
+    }
+  }
+  // Ascending eigenvalues, vectors permuted alike (through the spare matrix).
+  double* w = eps_of(base, n, v.ds);
+  double* T = mat(base, n, kt);
+  for (int i = tid; i < n; i += nt) {
+    const double wi = A[i * n + i];
+    int rk = 0;
+    for (int j = 0; j < n; ++j) {
+      const double wj = A[j * n + j];
+      if (wj < wi || (wj == wi && j < i)) ++rk;
+    }
+    w[rk] = wi;
+    for (int r2 = 0; r2 < n; ++r2) T[(size_t)r2 * n + rk] = V[(size_t)r2 * n + i];
+  }
+  __syncthreads();
+  for (int t = tid; t < n * n; t += nt) V[t] = T[t];
+}
+
+__global__ void k_copy(BatchView v, int ksrc, int kdst) {
+  BV_BEGIN();
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+    mat(base, n, kdst)[t] = mat(base, n, ksrc)[t];
+}
+
+// D = C_occ C_occ^T
+__global__ void k_density(BatchView v) {
+  BV_BEGIN();
+  const int nocc = ihdr(base)[I_NOCC];
+  const double* C = mat(base, n, M_C);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    double s = 0.0;
+    for (int k = 0; k < nocc; ++k) s += C[(size_t)r * n + k] * C[(size_t)c * n + k];
+    mat(base, n, M_D)[t] = s;
+  }
+}
+
+// tr(D X) into header slot hs (one block per molecule).
+__global__ void k_trace(BatchView v, int kx, int hs) {
+  const int b = blockIdx.x;
+  if (b >= v.nb || !v.active[b]) return;
+  const int n = v.nvec[b];
+  double* base = v.arena + v.region[b];
+  const double* D = mat(base, n, M_D);
+  const double* X = mat(base, n, kx);
+  double acc = 0.0;
+  for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) acc += D[t] * X[t];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+    base[hs] = s;
+  }
+}
+
+// E_elec = 2 sum_occ eps - tr(D G); iteration count, convergence (checkConvergence),
+// iteration cap; active flags for the next iteration; counts molecules still active.
+__global__ void k_energy(BatchView v, double conv, int max_iter, int* active_out, int* n_active) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb) return;
+  if (!v.active[b]) {
+    active_out[b] = 0;
+    return;
+  }
+  const int n = v.nvec[b];
+  double* base = v.arena + v.region[b];
+  int* ih = ihdr(base);
+  const double* w = eps_of(base, n, v.ds);
+  double e = 0.0;
+  for (int i = 0; i < ih[I_NOCC]; ++i) e += 2.0 * w[i];
+  e -= base[H_TRDG];
+  base[H_EPREV] = base[H_E];
+  base[H_E] = e;
+  ih[I_IT] += 1;
+  int act = 1;
+  if (!isfinite(e)) {
+    ih[I_DONE] = 1;
+    ih[I_STATUS] = DSS_ERR_NOCONV;
+    act = 0;
+  } else if (fabs(e - base[H_EPREV]) < conv) {
+    ih[I_DONE] = 1;
+    ih[I_STATUS] = DSS_OK;
+    act = 0;
+  } else if (ih[I_IT] >= max_iter) {
+    ih[I_DONE] = 1;
+    ih[I_STATUS] = DSS_ERR_NOCONV;
+    act = 0;
+  }
+  active_out[b] = act;
+  if (act) atomicAdd(n_active, 1);
+}
+
+// Final energy E = 2 tr(D H) + tr(D G) + E_nuc (calculateEnergies, Energy.cpp:21-50).
+__global__ void k_final(BatchView v) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb || !v.active[b]) return;
+  double* base = v.arena + v.region[b];
+  base[H_EFINAL] = 2.0 * base[H_TRDH] + base[H_TRDG] + base[H_ENUC];
+  ihdr(base)[I_FINAL] = 1;
+}
+
+// Admission set-up of one molecule's region (single block per matrix op).
+__global__ void k_admit_init(double* base, int n, const double* Hp, const double* Sp, const double* Dp, int nocc,
+                             double e_nuc) {
+  const long long n2 = (long long)n * n;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    const int x = r > c ? r : c, y = r > c ? c : r;
+    const long long pi = (long long)x * (x + 1) / 2 + y;
+    mat(base, n, M_H)[t] = Hp[pi];
+    mat(base, n, M_S)[t] = Sp[pi];
+    mat(base, n, M_T1)[t] = Sp[pi];
+    mat(base, n, M_D)[t] = Dp ? Dp[pi] : 0.0;
+    mat(base, n, M_CP)[t] = (r == c) ? 1.0 : 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int i = 0; i < kHdr; ++i) base[i] = 0.0;
+    base[H_ENUC] = e_nuc;
+    int* ih = ihdr(base);
+    ih[I_NOCC] = nocc;
+    ih[I_N] = n;
+  }
+}
+
+__global__ void k_scale_cols_inv_sqrt(const double* U, const double* w, double* out, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  out[t] = U[t] / sqrt(w[t % n]);
+}
+
+inline dim3 grid2(long long per_mol, int nb) {
+  long long bx = (per_mol + 255) / 256;
+  if (bx > 64) bx = 64;
+  if (bx < 1) bx = 1;
+  return dim3((unsigned)bx, (unsigned)nb);
+}
+
+}  // namespace
+
+struct dss_batch_mol {
+  bool live = false;
+  int n = 0, nocc = 0, natom = 0;
+  long long region = -1;
+  size_t size = 0;
+  BasisHost basis;  // molecule-local
+};
+
+struct dss_batch {
+  dss_ctx* ctx = nullptr;
+  std::string err;
+  int ds = 8;
+  DevBuf<double> arena;
+  size_t arena_doubles = 0;
+  std::vector<std::pair<size_t, size_t>> free_list;  // (offset, size) in doubles
+  std::vector<dss_batch_mol> mols;
+  bool dirty = true;
+  // current composition
+  std::vector<int> slot_mol;  // batch slot -> molecule handle
+  DevBuf<long long> d_region;
+  DevBuf<int> d_n, d_active, d_active_next, d_nact;
+  int nmax = 0;
+  int* h_nact = nullptr;  // pinned
+  cudaGraphExec_t graph = nullptr;
+  double graph_conv = -1.0;
+  int graph_maxit = -1;
+  ~dss_batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (h_nact) cudaFreeHost(h_nact);
+    if (ctx) dss_destroy(ctx);
+  }
+};
+
+namespace {
+
+int bfail(dss_batch* b, int code, const std::string& m) {
+  b->err = m;
+  return code;
+}
+
+bool arena_alloc(dss_batch* b, size_t want, size_t* off) {
+  for (size_t i = 0; i < b->free_list.size(); ++i) {
+    if (b->free_list[i].second >= want) {
+      *off = b->free_list[i].first;
+      b->free_list[i].first += want;
+      b->free_list[i].second -= want;
+      if (!b->free_list[i].second) b->free_list.erase(b->free_list.begin() + i);
+      return true;
+    }
+  }
+  return false;
+}
+
+void arena_free(dss_batch* b, size_t off, size_t size) {
+  b->free_list.push_back({off, size});
+  std::sort(b->free_list.begin(), b->free_list.end());
+  std::vector<std::pair<size_t, size_t>> merged;
+  for (auto& f : b->free_list) {
+    if (!merged.empty() && merged.back().first + merged.back().second == f.first) merged.back().second += f.second;
+    else merged.push_back(f);
+  }
+  b->free_list = merged;
+}
+
+BatchView view(dss_batch* b, const int* active) {
+  BatchView v;
+  v.arena = b->arena.ptr;
+  v.region = b->d_region.ptr;
+  v.nvec = b->d_n.ptr;
+  v.active = active;
+  v.nb = (int)b->slot_mol.size();
+  v.ds = b->ds;
+  return v;
+}
+
+// Rebuilds the batch basis (pairs, Schwarz factors, work lists) and the
+// per-slot tables for the live molecules.
+int rebuild(dss_batch* b) {
+  dss_ctx* ctx = b->ctx;
+  b->slot_mol.clear();
+  for (size_t h = 0; h < b->mols.size(); ++h)
+    if (b->mols[h].live) b->slot_mol.push_back((int)h);
+  const int nb = (int)b->slot_mol.size();
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (!nb) {
+    b->dirty = false;
+    return DSS_OK;
+  }
+  BasisHost B;
+  B.pure = b->mols[b->slot_mol[0]].basis.pure;
+  std::vector<long long> mbase, jbase, kbase, dbase;
+  std::vector<int> shn, shmol, shloc, shnsm;
+  std::vector<long long> region(nb);
+  std::vector<int> nv(nb);
+  long long dtot = 0;
+  b->nmax = 0;
+  for (int s = 0; s < nb; ++s) {
+    const dss_batch_mol& m = b->mols[b->slot_mol[s]];
+    const BasisHost& mb = m.basis;
+    region[s] = m.region;
+    nv[s] = m.n;
+    b->nmax = std::max(b->nmax, m.n);
+    const long long n2 = (long long)m.n * m.n;
+    const int ns = (int)mb.l.size();
+    const int p0 = (int)B.exps.size();
+    for (int q = 0; q < ns; ++q) {
+      B.l.push_back(mb.l[q]);
+      B.nprim.push_back(mb.nprim[q]);
+      B.prim0.push_back(p0 + mb.prim0[q]);
+      B.f0.push_back(mb.f0[q]);
+      for (int k = 0; k < 3; ++k) B.xyz.push_back(mb.xyz[3 * q + k]);
+      B.mol.push_back(s);
+      mbase.push_back(m.region + kHdr + (long long)M_DT * n2);
+      jbase.push_back(m.region + kHdr + (long long)M_J * n2);
+      kbase.push_back(m.region + kHdr + (long long)M_K * n2);
+      dbase.push_back(dtot);
+      shn.push_back(m.n);
+      shmol.push_back(s);
+      shloc.push_back(q);
+      shnsm.push_back(ns);
+    }
+    dtot += (long long)ns * ns;
+    B.exps.insert(B.exps.end(), mb.exps.begin(), mb.exps.end());
+    B.wts.insert(B.wts.end(), mb.wts.begin(), mb.wts.end());
+  }
+  B.nbf = 0;
+  ctx->nmol = nb;
+  ctx->basis = B;
+  int rc = dss_setup_pairs(ctx, std::move(B));
+  if (rc != DSS_OK) return bfail(b, rc, ctx->err);
+  ctx->nbf = 1;  // batch mode: accumulators are addressed per molecule
+  auto up = [&](auto& buf, const auto& host) -> int {
+    if (buf.resize(host.size()) != cudaSuccess) return DSS_ERR_OOM;
+    if (cudaMemcpyAsync(buf.ptr, host.data(), host.size() * sizeof(host[0]), cudaMemcpyHostToDevice, ctx->stream) !=
+        cudaSuccess)
+      return DSS_ERR_CUDA;
+    return DSS_OK;
+  };
+  if ((rc = up(ctx->d_sh_mbase, mbase)) || (rc = up(ctx->d_sh_jbase, jbase)) || (rc = up(ctx->d_sh_kbase, kbase)) ||
+      (rc = up(ctx->d_sh_dbase, dbase)) || (rc = up(ctx->d_sh_n, shn)) || (rc = up(ctx->d_sh_mol, shmol)) ||
+      (rc = up(ctx->d_sh_loc, shloc)) || (rc = up(ctx->d_sh_nsm, shnsm)) || (rc = up(b->d_region, region)) ||
+      (rc = up(b->d_n, nv)))
+    return bfail(b, rc, "batch: device tables");
+  if (b->d_active.resize(nb) != cudaSuccess || b->d_active_next.resize(nb) != cudaSuccess ||
+      b->d_nact.resize(1) != cudaSuccess)
+    return bfail(b, DSS_ERR_OOM, "batch: device tables");
+  b->dirty = false;
+  return DSS_OK;
+}
+
+__global__ void k_active_from_hdr(BatchView v, int* active, int want_final) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb) return;
+  int* ih = ihdr(v.arena + v.region[b]);
+  active[b] = want_final ? (ih[I_DONE] && !ih[I_FINAL]) : !ih[I_DONE];
+}
+
+// One SCF iteration for the active molecules (the captured body).
+int enqueue_iteration(dss_batch* b, double conv, int max_iter) {
+  dss_ctx* ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  const int nb = (int)b->slot_mol.size();
+  BatchView v = view(b, b->d_active.ptr);
+  const long long nn = (long long)b->nmax * b->nmax;
+  k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
+  ctx->d_mol_active = b->d_active.ptr;
+  BuildMode bm;
+  bm.boys = ctx->opts.boys_mode;
+  bm.no_zero = true;
+  int rc = dss_enqueue_jk(ctx, b->arena.ptr, b->arena.ptr, b->arena.ptr, nullptr, &bm);
+  if (rc != DSS_OK) return rc;
+  k_fock<<<grid2(nn, nb), 256, 0, s>>>(v);
+  const int tiles = (b->nmax + 31) / 32;
+  const dim3 gg(tiles, tiles, nb), gb(32, 8);
+  // DIIS error e = S D F_new - (S D F_new)^T
+  k_gemm<<<gg, gb, 0, s>>>(v, M_D, M_FN, M_T1, 0, 0, 1.0, 0.0);
+  k_gemm<<<gg, gb, 0, s>>>(v, M_S, M_T1, M_T2, 0, 0, 1.0, 0.0);
+  k_diis_choose<<<(nb + 127) / 128, 128, 0, s>>>(v);
+  k_diis_store<<<grid2(nn, nb), 256, 0, s>>>(v);
+  k_diis_dots<<<dim3(grid2(nn, nb).x, nb, b->ds), 256, 0, s>>>(v);
+  k_diis_solve<<<(nb + 127) / 128, 128, 0, s>>>(v);
+  k_diis_combine<<<grid2(nn, nb), 256, 0, s>>>(v);
+  // F' = X F X, rotated into the previous eigenvector basis: A = C'^T F' C'
+  k_gemm<<<gg, gb, 0, s>>>(v, M_F, M_X, M_T1, 0, 0, 1.0, 0.0);
+  k_gemm<<<gg, gb, 0, s>>>(v, M_X, M_T1, M_T2, 0, 0, 1.0, 0.0);
+  k_gemm<<<gg, gb, 0, s>>>(v, M_T2, M_CP, M_T1, 0, 0, 1.0, 0.0);
+  k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_T1, M_T2, 1, 0, 1.0, 0.0);
+  const size_t smem_full = (size_t)b->nmax * b->nmax * 8 + (size_t)(b->nmax + 2) * 8;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_jacobi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  if (smem_full <= 200 * 1024) {
+    k_jacobi<true><<<nb, 256, smem_full, s>>>(v, M_T2, M_V, M_T3, 40, 1e-15);
+  } else {
+    k_jacobi<false><<<nb, 256, (size_t)(b->nmax + 2) * 8, s>>>(v, M_T2, M_V, M_T3, 40, 1e-15);
+  }
+  // C' <- C' V (through T1), C = X C', D = C_occ C_occ^T
+  k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_V, M_T1, 0, 0, 1.0, 0.0);
+  k_copy<<<grid2(nn, nb), 256, 0, s>>>(v, M_T1, M_CP);
+  k_gemm<<<gg, gb, 0, s>>>(v, M_X, M_CP, M_C, 0, 0, 1.0, 0.0);
+  k_density<<<grid2(nn, nb), 256, 0, s>>>(v);
+  // E_elec = 2 sum eps_occ - tr(D G), G from the previous density
+  k_trace<<<nb, 256, 0, s>>>(v, M_G, H_TRDG);
+  if (cudaMemsetAsync(b->d_nact.ptr, 0, sizeof(int), s) != cudaSuccess) return DSS_ERR_CUDA;
+  k_energy<<<(nb + 127) / 128, 128, 0, s>>>(v, conv, max_iter, b->d_active_next.ptr, b->d_nact.ptr);
+  if (cudaMemcpyAsync(b->d_active.ptr, b->d_active_next.ptr, nb * sizeof(int), cudaMemcpyDeviceToDevice, s) !=
+      cudaSuccess)
+    return DSS_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return DSS_ERR_CUDA;
+  return DSS_OK;
+}
+
+// Final energies for molecules that finished but have no final energy yet.
+int finalize(dss_batch* b) {
+  dss_ctx* ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  const int nb = (int)b->slot_mol.size();
+  if (!nb) return DSS_OK;
+  BatchView v0 = view(b, b->d_active.ptr);
+  k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v0, b->d_active.ptr, 1);
+  BatchView v = view(b, b->d_active.ptr);
+  const long long nn = (long long)b->nmax * b->nmax;
+  k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
+  ctx->d_mol_active = b->d_active.ptr;
+  BuildMode bm;
+  bm.boys = ctx->opts.boys_mode;
+  bm.no_zero = true;
+  int rc = dss_enqueue_jk(ctx, b->arena.ptr, b->arena.ptr, b->arena.ptr, nullptr, &bm);
+  if (rc != DSS_OK) return rc;
+  k_fock<<<grid2(nn, nb), 256, 0, s>>>(v);
+  k_trace<<<nb, 256, 0, s>>>(v, M_H, H_TRDH);
+  k_trace<<<nb, 256, 0, s>>>(v, M_G, H_TRDG);
+  k_final<<<(nb + 127) / 128, 128, 0, s>>>(v);
+  if (cudaGetLastError() != cudaSuccess) return DSS_ERR_CUDA;
+  return DSS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dss_batch_create(dss_batch** out, const dss_opts* opts, size_t arena_bytes, int diis_size) {
+  if (!out) return DSS_ERR_INVALID;
+  *out = nullptr;
+  dss_batch* b = new (std::nothrow) dss_batch();
+  if (!b) return DSS_ERR_OOM;
+  int rc = dss_create(&b->ctx, opts);
+  if (rc != DSS_OK) {
+    delete b;
+    return rc;
+  }
+  b->ds = (diis_size >= 1 && diis_size <= 9) ? diis_size : 8;
+  if (!arena_bytes) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    arena_bytes = fr / 4;
+  }
+  b->arena_doubles = arena_bytes / 8;
+  if (b->arena.resize(b->arena_doubles) != cudaSuccess) {
+    delete b;
+    return DSS_ERR_OOM;
+  }
+  b->free_list.push_back({0, b->arena_doubles});
+  if (cudaMallocHost((void**)&b->h_nact, sizeof(int)) != cudaSuccess) {
+    delete b;
+    return DSS_ERR_OOM;
+  }
+  *out = b;
+  return DSS_OK;
+}
+
+void dss_batch_destroy(dss_batch* b) {
+  if (!b) return;
+  if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
+  delete b;
+}
+
+const char* dss_batch_last_error(const dss_batch* b) { return b ? b->err.c_str() : ""; }
+
+}  // extern "C"
+
+namespace {
+
+__global__ void k_pack_d(const double* D, double* p, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  if (r <= c) p[(long long)c * (c + 1) / 2 + r] = D[t];
+}
+
+int capture_graph(dss_batch* b, double conv, int max_iter) {
+  cudaStream_t s = b->ctx->stream;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return bfail(b, DSS_ERR_CUDA, "batch: stream capture failed to start");
+  const int rc = enqueue_iteration(b, conv, max_iter);
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc != DSS_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return bfail(b, DSS_ERR_CUDA, std::string("batch: graph capture: ") + cudaGetErrorString(e));
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("batch: graph instantiate: ") + cudaGetErrorString(ie));
+  b->graph_conv = conv;
+  b->graph_maxit = max_iter;
+  return DSS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,
+                  const double* centers, int pure, int natom, const int* Z, const double* xyz, int charge,
+                  const double* D_guess, int* handle) {
+  if (!b || !handle) return DSS_ERR_INVALID;
+  b->err.clear();
+  if (n_shell <= 0 || !l || !nprim || !exps || !coefs || !centers || natom <= 0 || !Z || !xyz)
+    return bfail(b, DSS_ERR_INVALID, "dss_batch_add: empty molecule or NULL array");
+  for (const auto& m : b->mols)
+    if (m.live && m.basis.pure != (pure ? 1 : 0))
+      return bfail(b, DSS_ERR_INVALID, "dss_batch_add: all molecules of a batch share the 5D/6D choice");
+  dss_batch_mol m;
+  std::string err;
+  int rc = dss_make_basis(n_shell, l, nprim, exps, coefs, centers, pure, &m.basis, &err);
+  if (rc != DSS_OK) return bfail(b, rc, err);
+  int ne = -charge;
+  for (int a = 0; a < natom; ++a) ne += Z[a];
+  if (ne < 0 || ne % 2) return bfail(b, DSS_ERR_INVALID, "dss_batch_add: closed-shell RHF needs an even electron count");
+  m.n = m.basis.nbf;
+  m.nocc = ne / 2;
+  m.natom = natom;
+  if (m.nocc > m.n) return bfail(b, DSS_ERR_INVALID, "dss_batch_add: more occupied orbitals than functions");
+  const size_t np = (size_t)m.n * (m.n + 1) / 2;
+  std::vector<double> S(np), T(np), V(np);
+  double e_nuc = 0.0;
+  rc = dss_one_electron_basis(m.basis, natom, Z, xyz, S.data(), T.data(), V.data(), &e_nuc, &err);
+  if (rc != DSS_OK) return bfail(b, rc, err);
+  for (size_t i = 0; i < np; ++i) T[i] += V[i];  // H
+  m.size = region_size(m.n, b->ds);
+  size_t off = 0;
+  if (!arena_alloc(b, m.size, &off))
+    return bfail(b, DSS_ERR_OOM, "dss_batch_add: not admitted, the batch arena has no room for this molecule");
+  m.region = (long long)off;
+  cudaStream_t s = b->ctx->stream;
+  cudaSetDevice(b->ctx->opts.device);
+  DevBuf<double> tmp;
+  const int n = m.n;
+  const size_t n2 = (size_t)n * n;
+  if (tmp.resize(3 * np + 4 * n2 + 128 + n) != cudaSuccess) {
+    arena_free(b, off, m.size);
+    return bfail(b, DSS_ERR_OOM, "dss_batch_add: device allocation failed");
+  }
+  double* dH = tmp.ptr;
+  double* dS = dH + np;
+  double* dD = dS + np;
+  double* work = dD + np;  // 3 n^2 + 64 + n
+  double* w = work + 3 * n2 + 64 + n;
+  cudaMemcpyAsync(dH, T.data(), np * 8, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dS, S.data(), np * 8, cudaMemcpyHostToDevice, s);
+  if (D_guess) cudaMemcpyAsync(dD, D_guess, np * 8, cudaMemcpyHostToDevice, s);
+  double* base = b->arena.ptr + off;
+  k_admit_init<<<(unsigned)std::min<size_t>((n2 + 255) / 256, 1024), 256, 0, s>>>(base, n, dH, dS,
+                                                                                  D_guess ? dD : nullptr, m.nocc,
+                                                                                  e_nuc);
+  // X = U s^-1/2 U^T from the eigen-decomposition of S (assignOrthogonalization).
+  double* A = base + kHdr + (size_t)M_T1 * n2;
+  double* U = base + kHdr + (size_t)M_V * n2;
+  double* X = base + kHdr + (size_t)M_X * n2;
+  double* T2 = base + kHdr + (size_t)M_T2 * n2;
+  cudaError_t e = dss_jacobi_eigh(s, n, A, U, w, work, 60, 1e-15, false);
+  if (e == cudaSuccess) {
+    k_scale_cols_inv_sqrt<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(U, w, T2, n);
+    dss_gemm(s, n, false, true, 1.0, T2, U, 0.0, X);
+    e = cudaStreamSynchronize(s);
+  }
+  if (e != cudaSuccess) {
+    arena_free(b, off, m.size);
+    return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_add: ") + cudaGetErrorString(e));
+  }
+  m.live = true;
+  b->mols.push_back(std::move(m));
+  *handle = (int)b->mols.size() - 1;
+  b->dirty = true;
+  return DSS_OK;
+}
+
+int dss_batch_step(dss_batch* b, const dss_scf_opts* opts, int iterations, int* n_active) {
+  if (!b) return DSS_ERR_INVALID;
+  b->err.clear();
+  dss_scf_opts o;
+  dss_default_scf_opts(&o);
+  if (opts) o = *opts;
+  cudaSetDevice(b->ctx->opts.device);
+  cudaStream_t s = b->ctx->stream;
+  bool fresh = false;
+  if (b->dirty) {
+    const int rc = rebuild(b);
+    if (rc != DSS_OK) return rc;
+    fresh = true;
+  }
+  const int nb = (int)b->slot_mol.size();
+  if (n_active) *n_active = 0;
+  if (!nb) return DSS_OK;
+  if (fresh) {
+    BatchView v = view(b, b->d_active.ptr);
+    k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v, b->d_active.ptr, 0);
+  }
+  int act = nb;
+  for (int it = 0; it < iterations && act > 0; ++it) {
+    if (!b->graph || b->graph_conv != o.conv || b->graph_maxit != o.max_iter) {
+      // First iteration after a change runs eagerly (sets kernel attributes), then capture.
+      int rc = enqueue_iteration(b, o.conv, o.max_iter);
+      if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: launch failed");
+      rc = capture_graph(b, o.conv, o.max_iter);
+      if (rc != DSS_OK) return rc;
+    } else {
+      if (cudaGraphLaunch(b->graph, s) != cudaSuccess) return bfail(b, DSS_ERR_CUDA, "dss_batch_step: graph launch");
+    }
+    cudaMemcpyAsync(b->h_nact, b->d_nact.ptr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_step: ") + cudaGetErrorString(e));
+    act = *b->h_nact;
+  }
+  const int rc = finalize(b);
+  if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: final energies");
+  // Restore the iteration flags for the next step.
+  BatchView v = view(b, b->d_active.ptr);
+  k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v, b->d_active.ptr, 0);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_step: ") + cudaGetErrorString(e));
+  if (n_active) *n_active = act;
+  return DSS_OK;
+}
+
+int dss_batch_solve(dss_batch* b, const dss_scf_opts* opts) {
+  dss_scf_opts o;
+  dss_default_scf_opts(&o);
+  if (opts) o = *opts;
+  int act = 0;
+  return dss_batch_step(b, &o, o.max_iter + 1, &act);
+}
+
+int dss_batch_result(dss_batch* b, int handle, double* E_total, double* D_packed, int* iterations, int* status) {
+  if (!b || handle < 0 || handle >= (int)b->mols.size() || !b->mols[handle].live) return DSS_ERR_INVALID;
+  const dss_batch_mol& m = b->mols[handle];
+  double hdr[kHdr];
+  cudaStream_t s = b->ctx->stream;
+  double* base = b->arena.ptr + m.region;
+  if (cudaMemcpyAsync(hdr, base, sizeof(hdr), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return bfail(b, DSS_ERR_CUDA, "dss_batch_result: copy");
+  const int* ih = reinterpret_cast<const int*>(hdr + H_INT);
+  if (!ih[I_FINAL]) return bfail(b, DSS_ERR_INVALID, "dss_batch_result: molecule not finished");
+  if (E_total) *E_total = hdr[H_EFINAL];
+  if (iterations) *iterations = ih[I_IT];
+  if (status) *status = ih[I_STATUS];
+  if (D_packed) {
+    const int n = m.n;
+    const size_t np = (size_t)n * (n + 1) / 2;
+    DevBuf<double> tmp;
+    if (tmp.resize(np) != cudaSuccess) return bfail(b, DSS_ERR_OOM, "dss_batch_result: allocation");
+    k_pack_d<<<(unsigned)(((size_t)n * n + 255) / 256), 256, 0, s>>>(base + kHdr + (size_t)M_D * n * n, tmp.ptr, n);
+    if (cudaMemcpyAsync(D_packed, tmp.ptr, np * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return bfail(b, DSS_ERR_CUDA, "dss_batch_result: copy D");
+  }
+  return DSS_OK;
+}
+
+int dss_batch_remove(dss_batch* b, int handle) {
+  if (!b || handle < 0 || handle >= (int)b->mols.size() || !b->mols[handle].live) return DSS_ERR_INVALID;
+  cudaStreamSynchronize(b->ctx->stream);
+  dss_batch_mol& m = b->mols[handle];
+  arena_free(b, (size_t)m.region, m.size);
+  m.live = false;
+  m.basis = BasisHost();
+  b->dirty = true;
+  return DSS_OK;
+}
+
+int dss_batch_info(const dss_batch* b, int* n_live, long long* free_bytes, long long* region_bytes_of_n) {
+  if (!b) return DSS_ERR_INVALID;
+  if (n_live) {
+    int c = 0;
+    for (const auto& m : b->mols) c += m.live ? 1 : 0;
+    *n_live = c;
+  }
+  if (free_bytes) {
+    size_t mx = 0;
+    for (const auto& f : b->free_list) mx = std::max(mx, f.second);
+    *free_bytes = (long long)mx * 8;
+  }
+  if (region_bytes_of_n && *region_bytes_of_n > 0) *region_bytes_of_n = (long long)region_size((int)*region_bytes_of_n, b->ds) * 8;
+  return DSS_OK;
+}
+
+int dss_batch_set_class_variant(dss_batch* b, int i, int variant) {
+  if (!b) return DSS_ERR_INVALID;
+  const int rc = dss_set_class_variant(b->ctx, i, variant);
+  if (rc == DSS_OK && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return rc;
+}
+
+void* dss_batch_context(dss_batch* b) { return b ? (void*)b->ctx : nullptr; }
+
+}  // extern "C"

@@ -182,20 +182,22 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
     const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
     if (!(x > thr)) m_series_lo = m;
   }
-  if (L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || m_series_lo > L || !(x > 1e-280) || !(x < 35.9)) {
-    boys_ref_series<L>(x, F);
-    return;
+  // Small x: the series is short (<= ~20 terms) and cheaper than the table path.
+  bool use_series = L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || m_series_lo > L || !(x >= 3.0) || !(x < 35.9);
+  int n = 1;
+  if (!use_series) {
+    // Truncation index of the m = L series.
+    const double* bp = g_boys_bp + L * (DSS_BOYS_NB + 1);
+    n = 1 + (int)g_boys_idx[L * DSS_BOYS_NG + (int)(x * 4.0)];
+    while (n <= DSS_BOYS_NB && bp[n] < x) ++n;
+    if (n > DSS_BOYS_NB) {
+      use_series = true;
+    } else {
+      const double lo_b = bp[n - 1], hi_b = bp[n];  // lo_b < x <= hi_b (bp[0] = 0)
+      use_series = fabs(x - hi_b) <= 4e-14 * x || fabs(x - lo_b) <= 4e-14 * x;
+    }
   }
-  // Truncation index of the m = L series.
-  const double* bp = g_boys_bp + L * (DSS_BOYS_NB + 1);
-  int n = 1 + (int)g_boys_idx[L * DSS_BOYS_NG + (int)(x * 4.0)];
-  while (n <= DSS_BOYS_NB && bp[n] < x) ++n;
-  if (n > DSS_BOYS_NB) {
-    boys_ref_series<L>(x, F);
-    return;
-  }
-  const double lo_b = bp[n - 1], hi_b = bp[n];  // lo_b < x <= hi_b (bp[0] = 0)
-  if (fabs(x - hi_b) <= 4e-14 * x || fabs(x - lo_b) <= 4e-14 * x) {
+  if (use_series) {
     boys_ref_series<L>(x, F);
     return;
   }
@@ -213,11 +215,13 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
   const double ex = exp(-x);
   const double x2 = 2.0 * x;
   const double tn = exp((double)n * log(x2) - g_boys_lp[L * (DSS_BOYS_NB + 1) + n]);
+  // Tail beyond the stop: terms fall geometrically; S >= 1, so terms below
+  // 1e-18 no longer change S at double precision.
   double tail = 0.0, t = tn;
-  for (int j = 1; j <= 64; ++j) {
+  for (int j = 1; j <= 48; ++j) {
     t = t * x2 * odd_inv(L + n + j);
     tail += t;
-    if (t < 1e-32) break;
+    if (t < 1e-18) break;
   }
   double S = fl * (double)(2 * L + 1) / ex - tail;
   double last = tn;

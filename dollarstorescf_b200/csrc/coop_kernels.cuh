@@ -103,13 +103,23 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
   if (k_begin >= k_end) return;  // uniform per warp
   const int bra = t.x;
   const int sa = __ldg(a.pair_a + bra), sb = __ldg(a.pair_b + bra);
-  const int n = a.n;
+  const double* __restrict__ Dm = a.D;
+  double* Jm = a.J;
+  double* Km = a.K;
+  int n = a.n;
+  if (a.sh_mbase) {  // batches: the bra pair fixes the molecule
+    if (a.mol_active && !__ldg(a.mol_active + __ldg(a.sh_mol + sa))) return;
+    n = __ldg(a.sh_n + sa);
+    Dm += __ldg(a.sh_mbase + sa);
+    Jm += __ldg(a.sh_jbase + sa);
+    Km += __ldg(a.sh_kbase + sa);
+  }
   const int fa = __ldg(a.sh_f0 + sa), fb = __ldg(a.sh_f0 + sb);
   const PrimPair* bpp = a.pp + __ldg(a.pair_pp0 + bra);
   const int nbp = __ldg(a.pair_npp + bra);
   for (int q = lane; q < NA * NB; q += 32) {
     jab[q] = 0.0;
-    dab[q] = __ldg(a.D + (size_t)(fa + q / NB) * n + fb + q % NB);
+    dab[q] = __ldg(Dm + (size_t)(fa + q / NB) * n + fb + q % NB);
   }
   const uint4* __restrict__ vrr = P::vrr();
   const uint4* __restrict__ accp = P::acc();
@@ -203,11 +213,11 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
     if (sa == sb) s *= 0.5;
     if (sc == sd) s *= 0.5;
     if (bra == ket) s *= 0.5;
-    for (int q = lane; q < NC * ND; q += 32) dcd[q] = __ldg(a.D + (size_t)(fc + q / ND) * n + fd + q % ND);
-    for (int q = lane; q < NA * ND; q += 32) dad[q] = __ldg(a.D + (size_t)(fa + q / ND) * n + fd + q % ND);
-    for (int q = lane; q < NB * ND; q += 32) dbd[q] = __ldg(a.D + (size_t)(fb + q / ND) * n + fd + q % ND);
-    for (int q = lane; q < NA * NC; q += 32) dac[q] = __ldg(a.D + (size_t)(fa + q / NC) * n + fc + q % NC);
-    for (int q = lane; q < NB * NC; q += 32) dbc[q] = __ldg(a.D + (size_t)(fb + q / NC) * n + fc + q % NC);
+    for (int q = lane; q < NC * ND; q += 32) dcd[q] = __ldg(Dm + (size_t)(fc + q / ND) * n + fd + q % ND);
+    for (int q = lane; q < NA * ND; q += 32) dad[q] = __ldg(Dm + (size_t)(fa + q / ND) * n + fd + q % ND);
+    for (int q = lane; q < NB * ND; q += 32) dbd[q] = __ldg(Dm + (size_t)(fb + q / ND) * n + fd + q % ND);
+    for (int q = lane; q < NA * NC; q += 32) dac[q] = __ldg(Dm + (size_t)(fa + q / NC) * n + fc + q % NC);
+    for (int q = lane; q < NB * NC; q += 32) dbc[q] = __ldg(Dm + (size_t)(fb + q / NC) * n + fc + q % NC);
     __syncwarp();
 #define DSS_I(i, j, k, l) vals[__ldg(outs + (((i) * NB + (j)) * NC + (k)) * ND + (l)) - 32u]
     // J over the bra pair: accumulated in shared memory across the task's kets.
@@ -223,39 +233,39 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
       double acc = 0.0;
       for (int i = 0; i < NA; ++i)
         for (int j = 0; j < NB; ++j) acc += DSS_I(i, j, k, l) * dab[i * NB + j];
-      atomicAdd(a.J + (size_t)(fc + k) * n + fd + l, 2.0 * s * acc);
+      atomicAdd(Jm + (size_t)(fc + k) * n + fd + l, 2.0 * s * acc);
     }
     for (int q = lane; q < NA * ND; q += 32) {  // K[i][l] += (ij|kl) D[j][k]
       const int i = q / ND, l = q % ND;
       double acc = 0.0;
       for (int j = 0; j < NB; ++j)
         for (int k = 0; k < NC; ++k) acc += DSS_I(i, j, k, l) * dbc[j * NC + k];
-      atomicAdd(a.K + (size_t)(fa + i) * n + fd + l, s * acc);
+      atomicAdd(Km + (size_t)(fa + i) * n + fd + l, s * acc);
     }
     for (int q = lane; q < NB * ND; q += 32) {  // K[j][l] += (ij|kl) D[i][k]
       const int j = q / ND, l = q % ND;
       double acc = 0.0;
       for (int i = 0; i < NA; ++i)
         for (int k = 0; k < NC; ++k) acc += DSS_I(i, j, k, l) * dac[i * NC + k];
-      atomicAdd(a.K + (size_t)(fb + j) * n + fd + l, s * acc);
+      atomicAdd(Km + (size_t)(fb + j) * n + fd + l, s * acc);
     }
     for (int q = lane; q < NA * NC; q += 32) {  // K[i][k] += (ij|kl) D[j][l]
       const int i = q / NC, k = q % NC;
       double acc = 0.0;
       for (int j = 0; j < NB; ++j)
         for (int l = 0; l < ND; ++l) acc += DSS_I(i, j, k, l) * dbd[j * ND + l];
-      atomicAdd(a.K + (size_t)(fa + i) * n + fc + k, s * acc);
+      atomicAdd(Km + (size_t)(fa + i) * n + fc + k, s * acc);
     }
     for (int q = lane; q < NB * NC; q += 32) {  // K[j][k] += (ij|kl) D[i][l]
       const int j = q / NC, k = q % NC;
       double acc = 0.0;
       for (int i = 0; i < NA; ++i)
         for (int l = 0; l < ND; ++l) acc += DSS_I(i, j, k, l) * dad[i * ND + l];
-      atomicAdd(a.K + (size_t)(fb + j) * n + fc + k, s * acc);
+      atomicAdd(Km + (size_t)(fb + j) * n + fc + k, s * acc);
     }
 #undef DSS_I
     __syncwarp();
   }
   for (int q = lane; q < NA * NB; q += 32)
-    atomicAdd(a.J + (size_t)(fa + q / NB) * n + fb + q % NB, 2.0 * jab[q]);
+    atomicAdd(Jm + (size_t)(fa + q / NB) * n + fb + q % NB, 2.0 * jab[q]);
 }

@@ -28,6 +28,16 @@ double dfact(int n) {
 
 int pair_class_index(int la, int lb) { return la * (la + 1) / 2 + lb; }
 
+// Primitive-pair screen: the pair's product overlap |w_a w_b| exp(-ab/p |AB|^2) (pi/p)^1.5.
+bool keep_prim_pair(const BasisHost& B, int a, int i, int b, int j, double ab2, double thr) {
+  if (thr <= 0.0) return true;
+  const double al = B.exps[B.prim0[a] + i], be = B.exps[B.prim0[b] + j];
+  const double p = al + be;
+  const double k = std::fabs(B.wts[B.prim0[a] + i] * B.wts[B.prim0[b] + j]) * std::exp(-al * be / p * ab2) *
+                   std::pow(kPiRef / p, 1.5);
+  return k >= thr;
+}
+
 __global__ void unpack_kernel(const double* __restrict__ packed, double* __restrict__ dense, int n) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n * n) return;
@@ -89,6 +99,47 @@ static int upload(dss_ctx* ctx, DevBuf<T>& buf, const std::vector<T>& host) {
   return DSS_OK;
 }
 
+int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,
+                   const double* centers, int pure, BasisHost* out, std::string* err) {
+  BasisHost B;
+  B.pure = pure ? 1 : 0;
+  int off = 0, f0 = 0;
+  for (int s = 0; s < n_shell; ++s) {
+    if (l[s] < 0 || l[s] > DSS_GEN_LMAX) {
+      *err = "dss_set_basis: angular momentum " + std::to_string(l[s]) + " above the compiled maximum " +
+             std::to_string(DSS_GEN_LMAX);
+      return DSS_ERR_UNSUPPORTED;
+    }
+    if (nprim[s] < 1 || nprim[s] > 100) {
+      *err = "dss_set_basis: Specified number of primitives (" + std::to_string(nprim[s]) +
+             ") is outside of the accepted range of 1-100.";
+      return DSS_ERR_INVALID;
+    }
+    B.l.push_back(l[s]);
+    B.nprim.push_back(nprim[s]);
+    B.prim0.push_back(off);
+    B.f0.push_back(f0);
+    for (int k = 0; k < 3; ++k) B.xyz.push_back(centers[3 * s + k]);
+    for (int p = 0; p < nprim[s]; ++p) {
+      const double zeta = exps[off + p];
+      if (!(zeta > 0.0)) {
+        *err = "dss_set_basis: Primitive GTOs must have positive exponents!";
+        return DSS_ERR_INVALID;
+      }
+      // chem/GTO.cpp:90-93, same operation order.
+      const double nf = (std::pow(2.0 * zeta, (double)l[s] + 1.5) * std::pow(2.0, (double)l[s] + 2)) /
+                        (std::sqrt(kPiRef) * dfact(2 * l[s] + 1));
+      B.exps.push_back(zeta);
+      B.wts.push_back(coefs[off + p] * std::sqrt(nf));
+    }
+    off += nprim[s];
+    f0 += pure ? 2 * l[s] + 1 : (l[s] + 1) * (l[s] + 2) / 2;
+  }
+  B.nbf = f0;
+  *out = std::move(B);
+  return DSS_OK;
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -97,6 +148,7 @@ void dss_default_opts(dss_opts* o) {
   o->device = 0;
   o->schwarz_threshold = 1e-12;
   o->boys_mode = DSS_BOYS_REF;
+  o->primitive_threshold = 1e-18;
 }
 
 int dss_create(dss_ctx** out, const dss_opts* opts) {
@@ -187,35 +239,11 @@ int dss_set_basis(dss_ctx* ctx, int n_shell, const int* l, const int* nprim, con
     return dss_fail(ctx, DSS_ERR_INVALID, "dss_set_basis: empty basis or NULL array");
   DSS_CUDA(cudaSetDevice(ctx->opts.device));
   BasisHost B;
-  B.pure = pure ? 1 : 0;
-  int off = 0, f0 = 0;
-  for (int s = 0; s < n_shell; ++s) {
-    if (l[s] < 0 || l[s] > DSS_GEN_LMAX)
-      return dss_fail(ctx, DSS_ERR_UNSUPPORTED,
-                      "dss_set_basis: angular momentum " + std::to_string(l[s]) + " above the compiled maximum " +
-                          std::to_string(DSS_GEN_LMAX));
-    if (nprim[s] < 1 || nprim[s] > 100)
-      return dss_fail(ctx, DSS_ERR_INVALID,
-                      "dss_set_basis: Specified number of primitives (" + std::to_string(nprim[s]) +
-                          ") is outside of the accepted range of 1-100.");
-    B.l.push_back(l[s]);
-    B.nprim.push_back(nprim[s]);
-    B.prim0.push_back(off);
-    B.f0.push_back(f0);
-    for (int k = 0; k < 3; ++k) B.xyz.push_back(centers[3 * s + k]);
-    for (int p = 0; p < nprim[s]; ++p) {
-      const double zeta = exps[off + p];
-      if (!(zeta > 0.0)) return dss_fail(ctx, DSS_ERR_INVALID, "dss_set_basis: Primitive GTOs must have positive exponents!");
-      // chem/GTO.cpp:90-93, same operation order.
-      const double nf = (std::pow(2.0 * zeta, (double)l[s] + 1.5) * std::pow(2.0, (double)l[s] + 2)) /
-                        (std::sqrt(kPiRef) * dfact(2 * l[s] + 1));
-      B.exps.push_back(zeta);
-      B.wts.push_back(coefs[off + p] * std::sqrt(nf));
-    }
-    off += nprim[s];
-    f0 += pure ? 2 * l[s] + 1 : (l[s] + 1) * (l[s] + 2) / 2;
-  }
-  B.nbf = f0;
+  std::string err;
+  const int mrc = dss_make_basis(n_shell, l, nprim, exps, coefs, centers, pure, &B, &err);
+  if (mrc != DSS_OK) return dss_fail(ctx, mrc, err);
+  ctx->nmol = 0;
+  ctx->d_mol_active = nullptr;
   ctx->basis = B;
   int rc = dss_setup_pairs(ctx, std::move(B));
   if (rc != DSS_OK) return rc;
@@ -290,19 +318,30 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
   const int ns = (int)B.l.size();
   // Unordered shell pairs {a, b}; stored with l_a >= l_b (ties: a >= b).
   struct PairTmp {
-    int a, b, cls, npp;
+    int a, b, cls, npp, mol;
   };
+  const bool batch = !B.mol.empty();
   std::vector<PairTmp> pairs;
   pairs.reserve((size_t)ns * (ns + 1) / 2);
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j <= i; ++j) {
+      if (batch && B.mol[i] != B.mol[j]) continue;  // pairs only inside a molecule
       int a = i, b = j;
       if (B.l[j] > B.l[i]) std::swap(a, b);
-      pairs.push_back({a, b, pair_class_index(B.l[a], B.l[b]), B.nprim[a] * B.nprim[b]});
+      // Primitive pairs kept by the primitive screen (same test as below).
+      int kept = 0;
+      const double dx = B.xyz[3 * a] - B.xyz[3 * b], dy = B.xyz[3 * a + 1] - B.xyz[3 * b + 1],
+                   dz = B.xyz[3 * a + 2] - B.xyz[3 * b + 2];
+      const double ab2 = dx * dx + dy * dy + dz * dz;
+      for (int p = 0; p < B.nprim[a]; ++p)
+        for (int q = 0; q < B.nprim[b]; ++q)
+          if (keep_prim_pair(B, a, p, b, q, ab2, ctx->opts.primitive_threshold)) ++kept;
+      pairs.push_back({a, b, pair_class_index(B.l[a], B.l[b]), kept, batch ? B.mol[a] : 0});
     }
-  // Order by class, then primitive-pair count (descending), then original order.
+  // Order by class, molecule, then primitive-pair count (descending), then original order.
   std::stable_sort(pairs.begin(), pairs.end(), [](const PairTmp& x, const PairTmp& y) {
     if (x.cls != y.cls) return x.cls < y.cls;
+    if (x.mol != y.mol) return x.mol < y.mol;
     return x.npp > y.npp;
   });
   const int np = (int)pairs.size();
@@ -319,6 +358,7 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
     const double ab2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
     for (int i = 0; i < B.nprim[a]; ++i)
       for (int j = 0; j < B.nprim[b]; ++j) {
+        if (!keep_prim_pair(B, a, i, b, j, ab2, ctx->opts.primitive_threshold)) continue;
         const double al = B.exps[B.prim0[a] + i], be = B.exps[B.prim0[b] + j];
         const double p = al + be;
         PrimPair r;
@@ -385,10 +425,11 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
   for (int q = 0; q < np; ++q) perm[q] = q;
   std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) {
     if (pairs[x].cls != pairs[y].cls) return pairs[x].cls < pairs[y].cls;
+    if (pairs[x].mol != pairs[y].mol) return pairs[x].mol < pairs[y].mol;
     if (pairs[x].npp != pairs[y].npp) return pairs[x].npp > pairs[y].npp;
     return Q[x] > Q[y];
   });
-  std::vector<int> pa2(np), pb2(np), p02(np), pn2(np), cls2(np);
+  std::vector<int> pa2(np), pb2(np), p02(np), pn2(np), cls2(np), mol2(np);
   std::vector<double> Q2(np);
   for (int q = 0; q < np; ++q) {
     const int o = perm[q];
@@ -397,6 +438,7 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
     p02[q] = p0[o];
     pn2[q] = pn[o];
     cls2[q] = pairs[o].cls;
+    mol2[q] = pairs[o].mol;
     Q2[q] = Q[o];
   }
   if ((rc = upload(ctx, ctx->d_pair_a, pa2)) != DSS_OK) return rc;
@@ -414,6 +456,7 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
   ctx->h_pair_b = pb2;
   ctx->h_pair_npp = pn2;
   ctx->h_pair_cls = cls2;
+  ctx->h_pair_mol = mol2;
   ctx->h_Q = Q2;
   ctx->class_pair0 = c0;
   ctx->class_pair1 = c1;
@@ -425,14 +468,25 @@ int dss_build_tasks(dss_ctx* ctx) {
   const double thr = ctx->opts.schwarz_threshold;
   const std::vector<double>& Q = ctx->h_Q;
   const std::vector<int>& npp = ctx->h_pair_npp;
-  // npp groups per class: [g0, g1) ranges with equal npp.
-  std::vector<std::vector<std::pair<int, int>>> groups(ncls);
+  const std::vector<int>& pmol = ctx->h_pair_mol;
+  // Groups per class: [g0, g1) ranges of one molecule with equal npp; per class
+  // and molecule the range of its groups.
+  struct Group {
+    int g0, g1, mol;
+  };
+  std::vector<std::vector<Group>> groups(ncls);
+  std::vector<std::vector<std::pair<int, int>>> mol_groups(ncls);
+  const int nm = ctx->nmol > 0 ? ctx->nmol : 1;
   for (int c = 0; c < ncls; ++c) {
+    mol_groups[c].assign(nm, {0, 0});
     int q = ctx->class_pair0[c];
     while (q < ctx->class_pair1[c]) {
       int e = q;
-      while (e < ctx->class_pair1[c] && npp[e] == npp[q]) ++e;
-      groups[c].push_back({q, e});
+      while (e < ctx->class_pair1[c] && npp[e] == npp[q] && pmol[e] == pmol[q]) ++e;
+      const int m = pmol[q];
+      if (mol_groups[c][m].second == 0) mol_groups[c][m] = {(int)groups[c].size(), (int)groups[c].size()};
+      groups[c].push_back({q, e, m});
+      mol_groups[c][m].second = (int)groups[c].size();
       q = e;
     }
   }
@@ -463,23 +517,25 @@ int dss_build_tasks(dss_ctx* ctx) {
     std::vector<int4> h;
     for (int ib = ctx->class_pair0[bc]; ib < ctx->class_pair1[bc]; ++ib) {
       const double Qb = Q[ib];
-      for (const auto& g : groups[kc]) {
-        int hi = g.second;
+      const std::pair<int, int> gr = mol_groups[kc][pmol[ib]];
+      for (int gi = gr.first; gi < gr.second; ++gi) {
+        const Group& g = groups[kc][gi];
+        int hi = g.g1;
         if (bc == kc) hi = std::min(hi, ib + 1);
-        if (hi <= g.first) continue;
-        // Q is descending in [g.first, hi): count the kets with Qb * Qk >= thr.
-        int lo_i = g.first, hi_i = hi;
+        if (hi <= g.g0) continue;
+        // Q is descending in [g.g0, hi): count the kets with Qb * Qk >= thr.
+        int lo_i = g.g0, hi_i = hi;
         while (lo_i < hi_i) {
           const int mid = (lo_i + hi_i) / 2;
           if (Qb * Q[mid] >= thr) lo_i = mid + 1;
           else hi_i = mid;
         }
-        const int nvalid = lo_i - g.first;
+        const int nvalid = lo_i - g.g0;
         for (int k0 = 0; k0 < nvalid; k0 += 32) {
           const int cnt = std::min(32, nvalid - k0);
-          h.push_back(make_int4(ib, g.first + k0, cnt, 0));
+          h.push_back(make_int4(ib, g.g0 + k0, cnt, pmol[ib]));
           ct.shell_quartets += cnt;
-          ct.prim_quartets += (long long)cnt * npp[ib] * npp[g.first];
+          ct.prim_quartets += (long long)cnt * npp[ib] * npp[g.g0];
         }
       }
     }
@@ -500,10 +556,13 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   BuildMode def;
   def.boys = ctx->opts.boys_mode;
   if (!mode) mode = &def;
+  const bool batch = ctx->nmol > 0;
   const int n = ctx->nbf;
   const size_t nn = (size_t)n * n;
-  DSS_CUDA(cudaMemsetAsync(Jacc, 0, nn * sizeof(double), ctx->stream));
-  DSS_CUDA(cudaMemsetAsync(Kacc, 0, nn * sizeof(double), ctx->stream));
+  if (!mode->no_zero) {
+    DSS_CUDA(cudaMemsetAsync(Jacc, 0, nn * sizeof(double), ctx->stream));
+    DSS_CUDA(cudaMemsetAsync(Kacc, 0, nn * sizeof(double), ctx->stream));
+  }
   // Launch order: highest total angular momentum first (longest per-quartet
   // latency), spread round-robin over the side streams; profiling (events)
   // keeps every launch on the main stream so each is timed alone.
@@ -524,7 +583,18 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   for (int ci : order) {
     ClassTasks& ct = ctx->tasks[ci];
     cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
-    EriArgs a;
+    EriArgs a{};
+    if (batch) {
+      a.sh_mbase = ctx->d_sh_mbase.ptr;
+      a.sh_jbase = ctx->d_sh_jbase.ptr;
+      a.sh_kbase = ctx->d_sh_kbase.ptr;
+      a.sh_n = ctx->d_sh_n.ptr;
+      a.sh_mol = ctx->d_sh_mol.ptr;
+      a.sh_loc = ctx->d_sh_loc.ptr;
+      a.sh_dbase = ctx->d_sh_dbase.ptr;
+      a.sh_nsm = ctx->d_sh_nsm.ptr;
+      a.mol_active = ctx->d_mol_active;
+    }
     a.tasks = ct.d_tasks.ptr;
     a.ntasks = ct.ntasks;
     a.pair_a = ctx->d_pair_a.ptr;

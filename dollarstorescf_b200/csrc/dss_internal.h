@@ -57,6 +57,7 @@ struct BasisHost {
   int nbf = 0;
   std::vector<int> l, nprim, prim0, f0;
   std::vector<double> xyz, exps, wts;
+  std::vector<int> mol;  // per shell: molecule of a batch (empty: one molecule); f0 is then molecule-local
 };
 
 struct ClassTasks {
@@ -97,6 +98,14 @@ struct dss_ctx {
   std::vector<int> class_pair0, class_pair1;
   std::vector<ClassTasks> tasks;
   std::vector<int> class_variant;  // per class: -1 default, 0 thread, 1 warp-cooperative
+  std::vector<int> h_pair_mol;
+
+  // Batch mode (nmol > 0, set by the batch engine): per-shell matrix offsets
+  // into the batch arena and per-molecule sizes; see EriArgs.
+  int nmol = 0;
+  DevBuf<long long> d_sh_mbase, d_sh_jbase, d_sh_kbase, d_sh_dbase;
+  DevBuf<int> d_sh_n, d_sh_mol, d_sh_loc, d_sh_nsm;
+  const int* d_mol_active = nullptr;
   long long n_shell_quartets = 0, n_prim_quartets = 0, n_warp_tasks = 0;
 
   // build scratch
@@ -115,6 +124,14 @@ struct dss_ctx {
     d_Qs.free();
     d_sh_nf.free();
     d_dmax.free();
+    d_sh_mbase.free();
+    d_sh_jbase.free();
+    d_sh_kbase.free();
+    d_sh_dbase.free();
+    d_sh_n.free();
+    d_sh_mol.free();
+    d_sh_loc.free();
+    d_sh_nsm.free();
     tasks.clear();
     nbf = 0;
   }
@@ -134,6 +151,12 @@ struct dss_ctx {
 int dss_fail(dss_ctx* ctx, int code, const std::string& msg);
 int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what);
 int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
+// Shells from the C-ABI arrays: validation and the reference's primitive normalisation.
+int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,
+                   const double* centers, int pure, BasisHost* out, std::string* err);
+// One-electron S, T, V (packed-U) and nuclear repulsion of one molecule's basis.
+int dss_one_electron_basis(const BasisHost& B, int natom, const int* Z, const double* xyz, double* S, double* T,
+                           double* V, double* e_nuc, std::string* err);
 int dss_build_tasks(dss_ctx* ctx);
 // G = (Jacc + Jacc^T) - (Kacc + Kacc^T) / 2, dense n x n.
 void dss_symmetrize_combine(cudaStream_t s, int n, const double* Jacc, const double* Kacc, double* G);
@@ -144,6 +167,7 @@ struct BuildMode {
   int mixed = 0;
   const float* dmax = nullptr;
   double skip_thr = 0.0, fp32_thr = 0.0;
+  bool no_zero = false;  // the caller has zeroed the accumulators (batch mode)
 };
 
 // Enqueues one J/K accumulation; with events != NULL records events[2i], events[2i+1]

@@ -43,6 +43,20 @@ struct EriArgs {
   const float* dmax;  // [nshell * nshell] max |D| per shell block
   int ns;
   double skip_thr, fp32_thr;
+  // Batches of molecules (NULL for one molecule): every shell carries the
+  // offsets of its molecule's n x n matrices from D, J and K, the molecule's n,
+  // its molecule index, its index among the molecule's shells, and the offset
+  // and shell count of the molecule's dmax block.  Quartets of molecules whose
+  // mol_active flag is 0 are skipped.
+  const long long* sh_mbase;
+  const long long* sh_jbase;
+  const long long* sh_kbase;
+  const int* sh_n;
+  const int* sh_mol;
+  const int* sh_loc;
+  const long long* sh_dbase;
+  const int* sh_nsm;
+  const int* mol_active;
 };
 
 struct SchwarzArgs {
@@ -90,7 +104,15 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Density bound of a quartet for the mixed-precision screen.
 __device__ __forceinline__ double quartet_dbound(const EriArgs& a, int sa, int sb, int sc, int sd) {
   const float* dm = a.dmax;
-  const int ns = a.ns;
+  int ns = a.ns;
+  if (a.sh_mbase) {
+    dm += a.sh_dbase[sa];
+    ns = a.sh_nsm[sa];
+    sa = a.sh_loc[sa];
+    sb = a.sh_loc[sb];
+    sc = a.sh_loc[sc];
+    sd = a.sh_loc[sd];
+  }
   float m = dm[sc * ns + sd];
   m = fmaxf(m, dm[sa * ns + sb]);
   m = fmaxf(m, dm[sa * ns + sd]);
@@ -113,6 +135,17 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(EriArgs a) {
   const int ket = t.y + (active ? lane : 0);
   const int sa = __ldg(a.pair_a + bra), sb = __ldg(a.pair_b + bra);
   const int sc = __ldg(a.pair_a + ket), sd = __ldg(a.pair_b + ket);
+  const double* __restrict__ Dm = a.D;
+  double* Jm = a.J;
+  double* Km = a.K;
+  int n = a.n;
+  if (a.sh_mbase) {  // uniform per warp: the bra pair fixes the molecule
+    if (a.mol_active && !__ldg(a.mol_active + __ldg(a.sh_mol + sa))) return;
+    n = __ldg(a.sh_n + sa);
+    Dm += __ldg(a.sh_mbase + sa);
+    Jm += __ldg(a.sh_jbase + sa);
+    Km += __ldg(a.sh_kbase + sa);
+  }
   bool fp32 = false;
   if constexpr (MIXED) {
     const double bound = __ldg(a.Qp + bra) * __ldg(a.Qp + ket) * quartet_dbound(a, sa, sb, sc, sd);
@@ -150,10 +183,9 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(EriArgs a) {
   if (sa == sb) s *= 0.5;
   if (sc == sd) s *= 0.5;
   if (bra == ket) s *= 0.5;
-  const int n = a.n;
   const int fa = __ldg(a.sh_f0 + sa), fb = __ldg(a.sh_f0 + sb);
   const int fc = __ldg(a.sh_f0 + sc), fd = __ldg(a.sh_f0 + sd);
-  const double* __restrict__ D = a.D;
+  const double* __restrict__ D = Dm;
 
   // Density blocks.
   double dab[NA * NB], dcd[NC * ND], dad[NA * ND], dbd[NB * ND], dac[NA * NC], dbc[NB * NC];
@@ -217,26 +249,26 @@ __global__ void __launch_bounds__(128) eri_jk_kernel(EriArgs a) {
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       const double v = warp_sum(jab[i * NB + j]);
-      if (lane == 0) atomicAdd(a.J + (size_t)(fa + i) * n + fb + j, 2.0 * v);
+      if (lane == 0) atomicAdd(Jm + (size_t)(fa + i) * n + fb + j, 2.0 * v);
     }
   if (active) {
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-      for (int l = 0; l < ND; ++l) atomicAdd(a.J + (size_t)(fc + k) * n + fd + l, 2.0 * jcd[k * ND + l]);
+      for (int l = 0; l < ND; ++l) atomicAdd(Jm + (size_t)(fc + k) * n + fd + l, 2.0 * jcd[k * ND + l]);
 #pragma unroll
     for (int i = 0; i < NA; ++i) {
 #pragma unroll
-      for (int l = 0; l < ND; ++l) atomicAdd(a.K + (size_t)(fa + i) * n + fd + l, kad[i * ND + l]);
+      for (int l = 0; l < ND; ++l) atomicAdd(Km + (size_t)(fa + i) * n + fd + l, kad[i * ND + l]);
 #pragma unroll
-      for (int k = 0; k < NC; ++k) atomicAdd(a.K + (size_t)(fa + i) * n + fc + k, kac[i * NC + k]);
+      for (int k = 0; k < NC; ++k) atomicAdd(Km + (size_t)(fa + i) * n + fc + k, kac[i * NC + k]);
     }
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
 #pragma unroll
-      for (int l = 0; l < ND; ++l) atomicAdd(a.K + (size_t)(fb + j) * n + fd + l, kbd[j * ND + l]);
+      for (int l = 0; l < ND; ++l) atomicAdd(Km + (size_t)(fb + j) * n + fd + l, kbd[j * ND + l]);
 #pragma unroll
-      for (int k = 0; k < NC; ++k) atomicAdd(a.K + (size_t)(fb + j) * n + fc + k, kbc[j * NC + k]);
+      for (int k = 0; k < NC; ++k) atomicAdd(Km + (size_t)(fb + j) * n + fc + k, kbc[j * NC + k]);
     }
   }
 }

@@ -208,13 +208,23 @@ extern "C" int dss_one_electron(dss_ctx* ctx, int natom, const int* Z, const dou
                                 double* T_packed, double* V_packed, double* e_nuc) {
   if (!ctx) return DSS_ERR_INVALID;
   ctx->err.clear();
-  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_one_electron: no basis set");
+  if (!ctx->nbf || ctx->nmol > 0) return dss_fail(ctx, DSS_ERR_INVALID, "dss_one_electron: no single-molecule basis set");
   if (natom < 0 || (natom > 0 && (!Z || !xyz_bohr)))
     return dss_fail(ctx, DSS_ERR_INVALID, "dss_one_electron: bad atom arrays");
-  const BasisHost& B = ctx->basis;
+  std::string err;
+  const int rc = dss_one_electron_basis(ctx->basis, natom, Z, xyz_bohr, S_packed, T_packed, V_packed, e_nuc, &err);
+  if (rc != DSS_OK) return dss_fail(ctx, rc, err);
+  return DSS_OK;
+}
+
+int dss_one_electron_basis(const BasisHost& B, int natom, const int* Z, const double* xyz_bohr, double* S_packed,
+                           double* T_packed, double* V_packed, double* e_nuc, std::string* errp) {
   const int ns = (int)B.l.size();
   for (int s = 0; s < ns; ++s)
-    if (B.l[s] > kLmax) return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_one_electron: l above 4");
+    if (B.l[s] > kLmax) {
+      if (errp) *errp = "dss_one_electron: l above 4";
+      return DSS_ERR_UNSUPPORTED;
+    }
   // Function transforms per (l, pure).
   std::vector<std::vector<std::vector<std::pair<int, double>>>> tr(kLmax + 1);
   for (int l = 0; l <= kLmax; ++l) tr[l].resize(B.pure ? 2 * l + 1 : ncart(l));

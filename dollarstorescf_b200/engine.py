@@ -30,9 +30,10 @@ def _ip(a: np.ndarray):
 
 
 class FockBuilder:
-    def __init__(self, device: int = 0, schwarz_threshold: float = 1e-12, boys_mode: int = BOYS_REF):
+    def __init__(self, device: int = 0, schwarz_threshold: float = 1e-12, boys_mode: int = BOYS_REF,
+                 primitive_threshold: float = 1e-18):
         self._L = _lib.load()
-        opts = _lib.DssOpts(device, schwarz_threshold, boys_mode)
+        opts = _lib.DssOpts(device, schwarz_threshold, boys_mode, primitive_threshold)
         h = ctypes.c_void_p()
         rc = self._L.dss_create(ctypes.byref(h), ctypes.byref(opts))
         if rc != 0:

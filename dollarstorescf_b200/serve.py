@@ -1,0 +1,157 @@
+"""Serving loop: continuous batching of SCF requests on one GPU.
+
+Requests (single points, or finite-difference displacements of a parent
+geometry warm-started from the parent's density, as the reference's frequency
+driver does, chem/scf/Frequency.cpp:121-133) arrive over time.  The loop admits
+every request that has arrived into the running batch while the batch arena has
+room (admission by device memory), runs SCF iterations of all admitted
+molecules together (dss_batch_step: one captured graph per iteration), and
+retires molecules as they finish, so new requests join while others are on the
+GPU.  Per request it records the latency from arrival to result.
+"""
+from __future__ import annotations
+
+import heapq
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import basis as basis_mod
+from . import geometry
+from .batch import Batch
+from .engine import BOYS_FAST, BOYS_REF, FockBuilder
+from .shells import ShellArrays, build_shells
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float  # seconds after the start of the stream
+    shells: ShellArrays
+    kind: str
+    guess: Optional[np.ndarray] = None  # packed-U alpha density of the parent
+
+
+@dataclass
+class Result:
+    rid: int
+    kind: str
+    energy: float
+    iterations: int
+    status: int
+    arrival: float
+    admitted: float
+    finished: float
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def poisson_arrivals(rate: float, count: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, count))
+
+
+def make_request_stream(count: int = 200, rate: float = 200.0, seed: int = 7, parent_density=None,
+                        dimer=None) -> List[Request]:
+    """The serving workload: 60% alkane single points (CnH2n+2, n ~ U{1..10},
+    STO-3G or 6-31G*), 40% +-0.005 bohr displacements of a water dimer
+    (6-31G*) along its 18 Cartesian coordinates, warm-started from the parent
+    density.  Everything is generated from the seed."""
+    rng = np.random.default_rng(seed)
+    times = poisson_arrivals(rate, count, seed + 1)
+    dimer = dimer if dimer is not None else geometry.water_dimer(seed)
+    disps = geometry.displacements(dimer, 0.005)
+    b631 = basis_mod.builtin_basis("6-31G*")
+    sto = basis_mod.builtin_basis("STO-3G")
+    out = []
+    for i, t in enumerate(times):
+        if rng.random() < 0.6:
+            n = int(rng.integers(1, 11))
+            bas = sto if rng.random() < 0.5 else b631
+            mol = geometry.alkane(n, int(rng.integers(0, 1 << 30)))
+            out.append(Request(i, float(t), build_shells(mol, bas, pure=True), f"alkane C{n} {bas.name}"))
+        else:
+            k = int(rng.integers(0, len(disps)))
+            out.append(Request(i, float(t), build_shells(disps[k], b631, pure=True), "dimer displacement",
+                               guess=parent_density))
+    return out
+
+
+def solve_parent(dimer, boys_mode: int = BOYS_REF, conv: float = 1e-10):
+    """The undisplaced water dimer, whose density warm-starts the displacements."""
+    sh = build_shells(dimer, basis_mod.builtin_basis("6-31G*"), pure=True)
+    with FockBuilder(schwarz_threshold=1e-12, boys_mode=boys_mode) as fb:
+        fb.set_basis(sh)
+        S, T, V, en = fb.one_electron(sh)
+        E, D, it, rc = fb.scf(T + V, S, sh.n_electrons() // 2, en, conv=conv)
+    return E, D
+
+
+def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boys_mode: int = BOYS_REF,
+          arena_bytes: int = 0, iterations_per_step: int = 1, realtime: bool = True,
+          batch: Optional[Batch] = None) -> Dict:
+    """Runs the request stream; returns per-request results and summary stats.
+    realtime=True replays arrivals against the wall clock; False admits each
+    request as soon as it is reached in arrival order (a closed loop)."""
+    own = batch is None
+    b = batch if batch is not None else Batch(schwarz_threshold=1e-12, boys_mode=boys_mode, arena_bytes=arena_bytes)
+    pending = sorted(requests, key=lambda r: r.arrival)
+    qi = 0
+    inflight: Dict[int, tuple] = {}
+    results: List[Result] = []
+    waiting: List[Request] = []
+    t0 = time.perf_counter()
+    peak_inflight = 0
+    admissions_deferred = 0
+    try:
+        while qi < len(pending) or waiting or inflight:
+            now = time.perf_counter() - t0
+            while qi < len(pending) and (pending[qi].arrival <= now or not realtime):
+                waiting.append(pending[qi])
+                qi += 1
+                if not realtime:
+                    break
+            # Admission: every waiting request that fits in the arena.
+            still = []
+            for r in waiting:
+                try:
+                    h = b.add(r.shells, guess=r.guess)
+                    inflight[h] = (r, time.perf_counter() - t0)
+                except Exception as e:  # arena full: wait for a slot to free up
+                    if getattr(e, "code", None) == -2:
+                        admissions_deferred += 1
+                        still.append(r)
+                    else:
+                        raise
+            waiting = still
+            peak_inflight = max(peak_inflight, len(inflight))
+            if not inflight:
+                if qi < len(pending) and realtime:
+                    time.sleep(max(0.0, pending[qi].arrival - (time.perf_counter() - t0)))
+                continue
+            b.step(iterations_per_step, conv=conv, max_iter=max_iter)
+            for h in list(inflight):
+                if b.finished(h):
+                    E, _, it, st = b.result(h)
+                    r, adm = inflight.pop(h)
+                    b.remove(h)
+                    results.append(Result(r.rid, r.kind, E, it, st, r.arrival, adm, time.perf_counter() - t0))
+    finally:
+        if own:
+            b.close()
+    wall = time.perf_counter() - t0
+    lat = np.array([r.latency for r in results])
+    return {
+        "results": results,
+        "solves": len(results),
+        "wall_s": wall,
+        "solves_per_s": len(results) / wall if wall > 0 else 0.0,
+        "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
+        "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
+        "peak_inflight": peak_inflight,
+        "admissions_deferred": admissions_deferred,
+    }

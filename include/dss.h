@@ -35,12 +35,14 @@ extern "C" {
 typedef struct dss_ctx dss_ctx;
 
 typedef struct dss_opts {
-  int device;               /* CUDA device ordinal */
-  double schwarz_threshold; /* drop shell quartets with Q_ab Q_cd below this (0: keep all) */
-  int boys_mode;            /* DSS_BOYS_REF or DSS_BOYS_FAST */
+  int device;                 /* CUDA device ordinal */
+  double schwarz_threshold;   /* drop shell quartets with Q_ab Q_cd below this (0: keep all) */
+  int boys_mode;              /* DSS_BOYS_REF or DSS_BOYS_FAST */
+  double primitive_threshold; /* drop primitive pairs with |K_ab| (pi/p)^1.5 below this (0: keep all) */
 } dss_opts;
 
-/* Defaults: device 0, Schwarz threshold 1e-12, reference Boys. */
+/* Defaults: device 0, Schwarz threshold 1e-12, reference Boys, primitive-pair
+ * threshold 1e-18 (each dropped pair changes any integral by < ~1e-15). */
 void dss_default_opts(dss_opts* opts);
 
 /* Creates a context on opts->device (opts may be NULL for the defaults).
@@ -179,6 +181,57 @@ void dss_default_scf_opts(dss_scf_opts* opts);
  * Returns DSS_ERR_NOCONV when max_iter is reached (outputs still written). */
 int dss_scf_solve(dss_ctx* ctx, const double* H_packed, const double* S_packed, int n_alpha, double e_nuc,
                   const dss_scf_opts* opts, double* E_total, double* D_alpha_inout, int* iterations);
+
+/* ---------------------------------------------------------------- batches of molecules */
+/* Many closed-shell molecules of uneven size solved together: each ERI class
+ * is one launch over every molecule of the batch, and one SCF iteration of all
+ * molecules (the steps of dss_scf_solve, plain form) is a captured CUDA graph
+ * whose per-molecule control (iteration count, DIIS ring, convergence) lives on
+ * the device.  Molecules may be added and removed between steps (continuous
+ * batching); each occupies a region of a device arena fixed at creation, and a
+ * molecule that does not fit is not admitted (DSS_ERR_OOM).  The reference has
+ * no batch mode; per molecule the iteration is the reference's solveMOs loop. */
+typedef struct dss_batch dss_batch;
+
+/* arena_bytes: device memory for molecule regions (0: a quarter of the free
+ * memory); diis_size 1..9 (0: 8). */
+int dss_batch_create(dss_batch** batch, const dss_opts* opts, size_t arena_bytes, int diis_size);
+void dss_batch_destroy(dss_batch* batch);
+const char* dss_batch_last_error(const dss_batch* batch);
+
+/* Admits one molecule (shells as in dss_set_basis, nuclei Z/xyz_bohr, total
+ * charge); D_guess (packed-U alpha density, may be NULL) warm-starts it, as the
+ * reference's frequency driver does by not resetting the density
+ * (chem/scf/Frequency.cpp:121-133).  *handle identifies it. */
+int dss_batch_add(dss_batch* batch, int n_shell, const int* l, const int* nprim, const double* exps,
+                  const double* coefs, const double* centers_bohr, int pure, int natom, const int* Z,
+                  const double* xyz_bohr, int charge, const double* D_guess, int* handle);
+
+/* Runs up to `iterations` SCF iterations of every unfinished molecule, then
+ * computes the final energies of those that finished.  *n_active: molecules
+ * still iterating. */
+int dss_batch_step(dss_batch* batch, const dss_scf_opts* opts, int iterations, int* n_active);
+
+/* Steps until every molecule finished (converged or reached max_iter). */
+int dss_batch_solve(dss_batch* batch, const dss_scf_opts* opts);
+
+/* Result of a finished molecule: total energy, final alpha density (packed-U,
+ * may be NULL), iterations, status (DSS_OK or DSS_ERR_NOCONV). */
+int dss_batch_result(dss_batch* batch, int handle, double* E_total, double* D_packed, int* iterations,
+                     int* status);
+
+/* Releases a molecule's region. */
+int dss_batch_remove(dss_batch* batch, int handle);
+
+/* Live molecules, largest free arena block in bytes, and (in/out) the region
+ * bytes a molecule of *region_bytes_of_n functions needs. */
+int dss_batch_info(const dss_batch* batch, int* n_live, long long* free_bytes, long long* region_bytes_of_n);
+
+/* Kernel variant of class i for the batch (see dss_set_class_variant). */
+int dss_batch_set_class_variant(dss_batch* batch, int i, int variant);
+
+/* The batch's Fock-build context (for dss_class_info / dss_get_class_variant). */
+void* dss_batch_context(dss_batch* batch);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,63 @@
+"""Batched form: many molecules of uneven size in one set of launches, each
+molecule's energy equal to the reference's (golden) and to its energy when
+solved alone; molecules joining and leaving between iterations."""
+import numpy as np
+import pytest
+
+from conftest import load_case
+from dollarstorescf_b200.batch import Batch
+from dollarstorescf_b200.engine import BOYS_REF
+
+pytestmark = pytest.mark.gpu
+
+MIX = ["water_sto3g", "water_631g", "ch4_631g", "c3h8_sto3g", "water_631gs", "dimer_631gs", "he_631g"]
+
+
+def test_batch_energies_match_reference_and_alone():
+    cases = [load_case(n) for n in MIX]
+    with Batch(schwarz_threshold=0.0, boys_mode=BOYS_REF) as b:
+        hs = [b.add(sh) for (_, _, sh) in cases]
+        b.solve(conv=1e-10)
+        mixed = [b.result(h)[0] for h in hs]
+    for (d, _, _), E in zip(cases, mixed):
+        assert abs(E - float(d["E"])) < 1e-9, (E, float(d["E"]))
+    # alone
+    for (d, _, sh), Em in zip(cases, mixed):
+        with Batch(schwarz_threshold=0.0, boys_mode=BOYS_REF) as b:
+            h = b.add(sh)
+            b.solve(conv=1e-10)
+            Ea = b.result(h)[0]
+        assert abs(Ea - Em) < 1e-10
+
+
+def test_batch_continuous_join_and_leave():
+    d1, _, sh1 = load_case("water_631gs")
+    d2, _, sh2 = load_case("ch4_631g")
+    d3, _, sh3 = load_case("dimer_631gs")
+    with Batch(schwarz_threshold=0.0, boys_mode=BOYS_REF) as b:
+        h1 = b.add(sh1)
+        h2 = b.add(sh2)
+        b.step(3, conv=1e-10)          # both under way
+        h3 = b.add(sh3)                # joins mid-flight
+        done = {}
+        for _ in range(200):
+            act = b.step(1, conv=1e-10)
+            for h in (h1, h2, h3):
+                if h not in done and b.finished(h):
+                    done[h] = b.result(h)[0]
+                    b.remove(h)        # leaves; the others keep iterating
+            if len(done) == 3:
+                break
+        assert len(done) == 3
+    assert abs(done[h1] - float(d1["E"])) < 1e-9
+    assert abs(done[h2] - float(d2["E"])) < 1e-9
+    assert abs(done[h3] - float(d3["E"])) < 1e-9
+
+
+def test_batch_admission_by_memory():
+    d, _, sh = load_case("dimer_631gs")
+    with Batch(arena_bytes=600_000) as b:   # one 36-function molecule needs about 0.33 MB: one fits, two do not
+        b.add(sh)
+        with pytest.raises(Exception) as e:
+            b.add(sh)
+        assert "not admitted" in str(e.value)
