@@ -95,6 +95,12 @@ class FockBuilder:
         self._check(self._L.dss_build_jk_device(self._h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(J_ptr),
                                                 ctypes.c_void_p(K_ptr)))
 
+    def jk_device_noalloc(self, D_ptr: int, J_ptr: int, K_ptr: int) -> None:
+        """Same build as jk_device with the accumulators in the library's fixed
+        device array: no device allocation in the call (n <= 512)."""
+        self._check(self._L.dss_build_jk_device_noalloc(self._h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(J_ptr),
+                                                        ctypes.c_void_p(K_ptr)))
+
     def jk_host_ptrs(self, D_ptr: int, J_ptr: int, K_ptr: int) -> None:
         """dss_build_jk on raw host pointers (e.g. pinned buffers)."""
         self._check(self._L.dss_build_jk(self._h, ctypes.cast(D_ptr, ctypes.POINTER(ctypes.c_double)),
