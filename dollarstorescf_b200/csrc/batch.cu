@@ -719,9 +719,9 @@ int enqueue_iteration(dss_batch* b, double conv, int max_iter) {
     attr = true;
   }
   if (smem_full <= 200 * 1024) {
-    k_jacobi<true><<<nb, 256, smem_full, s>>>(v, M_T2, M_V, M_T3, 40, 1e-15);
+    k_jacobi<true><<<nb, 256, smem_full, s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL);
   } else {
-    k_jacobi<false><<<nb, 256, (size_t)(b->nmax + 2) * 8, s>>>(v, M_T2, M_V, M_T3, 40, 1e-15);
+    k_jacobi<false><<<nb, 256, (size_t)(b->nmax + 2) * 8, s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL);
   }
   // C' <- C' V (through T1), C = X C', D = C_occ C_occ^T
   k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_V, M_T1, 0, 0, 1.0, 0.0);
@@ -903,7 +903,7 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   double* U = base + kHdr + (size_t)M_V * n2;
   double* X = base + kHdr + (size_t)M_X * n2;
   double* T2 = base + kHdr + (size_t)M_T2 * n2;
-  cudaError_t e = dss_jacobi_eigh(s, n, A, U, w, work, 60, 1e-15, false);
+  cudaError_t e = dss_jacobi_eigh(s, n, A, U, w, work, 60, DSS_JACOBI_TOL, false);
   if (e == cudaSuccess) {
     k_scale_cols_inv_sqrt<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(U, w, T2, n);
     dss_gemm(s, n, false, true, 1.0, T2, U, 0.0, X);

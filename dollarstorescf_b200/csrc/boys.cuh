@@ -182,8 +182,9 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
     const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
     if (!(x > thr)) m_series_lo = m;
   }
-  // Small x: the series is short (<= ~20 terms) and cheaper than the table path.
-  bool use_series = L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || m_series_lo > L || !(x >= 3.0) || !(x < 35.9);
+  // One code path for all lanes of a warp (their x differ): the series runs only
+  // for orders outside the tables, x ~ 0, x beyond the table, or all-asymptotic.
+  bool use_series = L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || m_series_lo > L || !(x > 1e-280) || !(x < 35.9);
   int n = 1;
   if (!use_series) {
     // Truncation index of the m = L series.
@@ -215,13 +216,15 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
   const double ex = exp(-x);
   const double x2 = 2.0 * x;
   const double tn = exp((double)n * log(x2) - g_boys_lp[L * (DSS_BOYS_NB + 1) + n]);
-  // Tail beyond the stop: terms fall geometrically; S >= 1, so terms below
-  // 1e-18 no longer change S at double precision.
+  // Tail beyond the stop: t_n <= 1e-9 and the term ratio 2x/(2L+2n+2j+1) is at
+  // most 0.37 there for every x < 36, so 20 further terms reach below 2e-18,
+  // where they no longer change S (S >= 1) at double precision.  A fixed trip
+  // count keeps the warp's lanes together.
   double tail = 0.0, t = tn;
-  for (int j = 1; j <= 48; ++j) {
+#pragma unroll
+  for (int j = 1; j <= 20; ++j) {
     t = t * x2 * odd_inv(L + n + j);
     tail += t;
-    if (t < 1e-18) break;
   }
   double S = fl * (double)(2 * L + 1) / ex - tail;
   double last = tn;

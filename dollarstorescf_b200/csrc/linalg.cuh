@@ -4,6 +4,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+// Jacobi stops when the off-diagonal Frobenius norm is below this fraction of
+// the whole; double rounding leaves a floor near sqrt(n) * 1.1e-16 (2.7e-15 at
+// n = 608), so a tighter target would only burn sweeps.
+#define DSS_JACOBI_TOL 1e-14
+
 // C = alpha * op(A) * op(B) + beta * C, op = transpose when the flag is set.
 void dss_gemm(cudaStream_t s, int n, bool ta, bool tb, double alpha, const double* A, const double* B, double beta,
               double* C);

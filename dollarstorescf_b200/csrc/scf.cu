@@ -292,7 +292,7 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
   unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, S, n);
   // X = U s^-1/2 U^T from the eigen-decomposition of S (assignOrthogonalization).
   SCF_CHECK(cudaMemcpyAsync(T1, S, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy S");
-  SCF_CHECK(dss_jacobi_eigh(s, n, T1, T2, eps, work, 60, 1e-15, false), "eigh(S)");
+  SCF_CHECK(dss_jacobi_eigh(s, n, T1, T2, eps, work, 60, DSS_JACOBI_TOL, false), "eigh(S)");
   scale_cols<<<nb(n2), 256, 0, s>>>(T2, eps, T1, n, 1);
   dss_gemm(s, n, false, true, 1.0, T1, T2, 0.0, X);
   // Initial density.
@@ -378,11 +378,11 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
     if (have_cp) {
       dss_gemm(s, n, false, false, 1.0, T2, Cp, 0.0, T1);
       dss_gemm(s, n, true, false, 1.0, Cp, T1, 0.0, T2);  // Cp^T F' Cp
-      SCF_CHECK(dss_jacobi_eigh(s, n, T2, T1, eps, work, 40, 1e-15, false), "eigh(F')");
+      SCF_CHECK(dss_jacobi_eigh(s, n, T2, T1, eps, work, 40, DSS_JACOBI_TOL, false), "eigh(F')");
       dss_gemm(s, n, false, false, 1.0, Cp, T1, 0.0, T2);
       SCF_CHECK(cudaMemcpyAsync(Cp, T2, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy C'");
     } else {
-      SCF_CHECK(dss_jacobi_eigh(s, n, T2, Cp, eps, work, 60, 1e-15, false), "eigh(F')");
+      SCF_CHECK(dss_jacobi_eigh(s, n, T2, Cp, eps, work, 60, DSS_JACOBI_TOL, false), "eigh(F')");
       have_cp = true;
     }
     dss_gemm(s, n, false, false, 1.0, X, Cp, 0.0, C);

@@ -27,7 +27,7 @@ def load_case(name):
 
 
 GOLDEN_CASES = ["water_sto3g", "water_sto3g_6d", "water_631g", "water_631gs", "water_631gs_6d",
-                "dimer_631gs", "dimer_631gs_6d", "ch4_631g", "c3h8_sto3g", "w4_631gs", "he_631g",
+                "dimer_631gs", "dimer_631gs_6d", "ch4_631g", "c3h8_sto3g", "w4_631gs", "w8_631gs", "he_631g",
                 "h2_631g", "testwater_631gs"]
 
 

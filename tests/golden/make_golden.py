@@ -8,7 +8,8 @@ oracle/build_ref.sh and driven through oracle/ref_harness.cpp:
                    J[D_total], K[D_alpha] and G = J - K at that density, the
                    same three for a seeded random symmetric density, S and H.
 
-Usage (in a container with /root/reference): python tests/golden/make_golden.py
+Usage (in a container with /root/reference): python tests/golden/make_golden.py [case ...]
+(with case names: only those fixtures; (H2O)8 takes several minutes)
 """
 from __future__ import annotations
 
@@ -39,6 +40,7 @@ def cases():
         ("ch4_631g", geometry.alkane(1, 0), "6-31G", True),
         ("c3h8_sto3g", geometry.alkane(3, 1), "STO-3G", True),
         ("w4_631gs", geometry.water_cluster(2, 2, 1, 4, 0), "6-31G*", True),
+        ("w8_631gs", geometry.water_cluster(2, 2, 2, 8, 5), "6-31G*", True),
     ]
     for name, xyz, bas in (("he_631g", "He.xyz", "6-31G"), ("h2_631g", "hydrogen.xyz", "6-31G"),
                            ("testwater_631gs", "water.xyz", "6-31G*")):
@@ -47,25 +49,36 @@ def cases():
 
 
 def main() -> None:
+    only = set(sys.argv[1:])
+    if only:
+        rng = np.random.default_rng(1234)
+        for name, mol, bas, pure in cases():
+            if name in only:
+                write_case(name, mol, bas, pure, rng)
+        return
     xs = np.concatenate([[0.0, 1e-12, 1e-9, 1e-6, 1e-3], np.linspace(0.01, 40.0, 397), [24.99, 25.0, 25.01, 26.1, 26.2]])
     ms = np.arange(0, 13)
     tab = np.array([[refpy.boys(float(x), int(m)) for m in ms] for x in xs])
     np.savez_compressed(os.path.join(HERE, "boys_ref.npz"), x=xs, m=ms, F=tab)
     rng = np.random.default_rng(1234)
     for name, mol, bas, pure in cases():
-        sh = shells.build_shells(mol, basis.builtin_basis(bas), pure=pure)
-        n = refpy.setup(sh)
-        E, D, it, secs = refpy.scf(1e-10)
-        J, K = refpy.jk(D)
-        G = refpy.fock_2e(D)
-        A = rng.standard_normal((n, n)) * 0.1
-        Dr = shells.pack(A + A.T)
-        Jr, Kr = refpy.jk(Dr)
-        np.savez_compressed(
-            os.path.join(HERE, name + ".npz"), Z=np.asarray(mol.Z), xyz=np.asarray(mol.xyz), basis=bas,
-            pure=pure, nbf=n, E=E, iterations=it, D=D, J=J, K=K, G=G, D_rand=Dr, J_rand=Jr, K_rand=Kr,
-            S=refpy.overlap(), H=refpy.core_hamiltonian(), e_nuc=mol.nuclear_repulsion())
-        print(f"{name:18s} n={n:4d} E={E:.13f} it={it} ({secs:.2f}s)")
+        write_case(name, mol, bas, pure, rng)
+
+
+def write_case(name, mol, bas, pure, rng) -> None:
+    sh = shells.build_shells(mol, basis.builtin_basis(bas), pure=pure)
+    n = refpy.setup(sh)
+    E, D, it, secs = refpy.scf(1e-10)
+    J, K = refpy.jk(D)
+    G = refpy.fock_2e(D)
+    A = rng.standard_normal((n, n)) * 0.1
+    Dr = shells.pack(A + A.T)
+    Jr, Kr = refpy.jk(Dr)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"), Z=np.asarray(mol.Z), xyz=np.asarray(mol.xyz), basis=bas,
+        pure=pure, nbf=n, E=E, iterations=it, D=D, J=J, K=K, G=G, D_rand=Dr, J_rand=Jr, K_rand=Kr,
+        S=refpy.overlap(), H=refpy.core_hamiltonian(), e_nuc=mol.nuclear_repulsion())
+    print(f"{name:18s} n={n:4d} E={E:.13f} it={it} ({secs:.2f}s)")
 
 
 if __name__ == "__main__":
