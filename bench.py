@@ -33,6 +33,7 @@ import math
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -133,7 +134,8 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "_build",
+        # DSS_CLOCKS_DIR keeps the raw nvidia-smi samples where the caller wants them.
+        self.path = os.path.join(os.environ.get("DSS_CLOCKS_DIR") or tempfile.gettempdir(),
                                  f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
@@ -345,11 +347,113 @@ def run_gpu(args):
         if r is not None:
             line["cpu_baseline"] = {"value": r[0], "unit": "builds/s", "cores": r[2], "kind": "reference",
                                     "sample": r[3]}
+    fb.close()
+    if rank == 0 and not args.no_forms:
+        line["forms"] = measure_forms(device, args.forms_molecules, args.forms_requests)
     if rank == 0:
         print(json.dumps(line))
-    fb.close()
     if ws > 1:
         dist.destroy_process_group()
+
+
+def measure_forms(device: int, n_alkanes: int, n_requests: int):
+    """SCF solves/s of the plain FP64 GPU form against the mixed-precision,
+    batched and served forms, wall-clock timed around each call (each returns
+    only after its results are on the host), with per-molecule |dE| of every
+    mixed result against the FP64 result of the same molecule.
+
+      scf_h2o32   (H2O)32 6-31G* 6D (608 functions): dss_scf_solve plain
+                  (reference Boys, full FP64 build every iteration) vs the
+                  incremental mixed-precision form (FP32 below 1e-7).
+      alkanes     n_alkanes seeded CnH2n+2 (n ~ U{1..10}) 6-31G, conv 1e-10,
+                  64-iteration cap.  plain_sequential: one dss_scf_solve per
+                  molecule (first 16); batched_fp64 / batched_mixed: one
+                  dss_batch for all of them.
+      serve       n_requests at a Poisson 200 req/s (60% alkanes STO-3G /
+                  6-31G*, 40% water-dimer 6-31G* displacements warm-started from
+                  the parent density), continuous batching in the FP64 and the
+                  mixed form; plain_sequential: dss_scf_solve over the first 16.
+    """
+    import time as _t
+
+    import numpy as np
+
+    from dollarstorescf_b200 import basis as B
+    from dollarstorescf_b200 import geometry, serve, shells
+    from dollarstorescf_b200.batch import Batch
+    from dollarstorescf_b200.engine import BOYS_REF, FockBuilder
+
+    def solve_plain(shs, guesses=None):
+        t0 = _t.perf_counter()
+        ok = 0
+        for i, s in enumerate(shs):
+            with FockBuilder(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as fb:
+                fb.set_basis(s)
+                S, T, V, en = fb.one_electron(s)
+                g = guesses[i] if guesses is not None else None
+                E, D, it, rc = fb.scf(T + V, S, s.n_electrons() // 2, en, conv=1e-10, max_iter=64, guess=g,
+                                      raise_on_noconv=False)
+                ok += rc == 0
+        return {"solves_per_s": len(shs) / (_t.perf_counter() - t0), "sample": len(shs), "converged": ok}
+
+    out = {}
+    w32 = geometry.water_cluster(4, 4, 2, 32, seed=2024)
+    sh32 = shells.build_shells(w32, B.builtin_basis("6-31G*"), pure=False)
+    with FockBuilder(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as fb:
+        fb.set_basis(sh32)
+        S, T, V, en = fb.one_electron(sh32)
+        ne = sh32.n_electrons() // 2
+        res = {"nbf": sh32.nbf()}
+        for mode in ("plain", "mixed"):
+            t0 = _t.perf_counter()
+            E, D, it, rc = fb.scf(T + V, S, ne, en, conv=1e-10, mixed=(mode == "mixed"), fp32_threshold=1e-7)
+            dt = _t.perf_counter() - t0
+            res[mode] = {"solves_per_s": 1.0 / dt, "iterations": it, "energy": E, "status": rc}
+        res["mixed"]["abs_dE_vs_fp64"] = abs(res["mixed"]["energy"] - res["plain"]["energy"])
+        res["mixed_over_plain"] = res["mixed"]["solves_per_s"] / res["plain"]["solves_per_s"]
+        out["scf_h2o32"] = res
+
+    rng = np.random.default_rng(4)
+    alk = [shells.build_shells(geometry.alkane(int(rng.integers(1, 11)), i), B.builtin_basis("6-31G"), pure=True)
+           for i in range(n_alkanes)]
+    ares = {"molecules": n_alkanes, "conv": 1e-10, "max_iter": 64,
+            "plain_sequential": solve_plain(alk[:min(16, n_alkanes)])}
+    energies = {}
+    for name, mixed in (("batched_fp64", False), ("batched_mixed", True)):
+        with Batch(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as b:
+            t0 = _t.perf_counter()
+            hs = [b.add(s) for s in alk]
+            b.solve(conv=1e-10, max_iter=64, mixed=mixed)
+            dt = _t.perf_counter() - t0
+            r = [b.result(h) for h in hs]
+        energies[name] = [(x[0], x[3]) for x in r]
+        ares[name] = {"solves_per_s": len(alk) / dt, "converged": int(sum(1 for x in r if x[3] == 0)),
+                      "wall_s": dt}
+    both = [(a[0], m[0]) for a, m in zip(energies["batched_fp64"], energies["batched_mixed"]) if a[1] == 0 and m[1] == 0]
+    ares["batched_mixed"]["max_abs_dE_vs_fp64"] = max(abs(a - m) for a, m in both) if both else None
+    base = ares["plain_sequential"]["solves_per_s"]
+    ares["batched_fp64_over_plain"] = ares["batched_fp64"]["solves_per_s"] / base
+    ares["batched_mixed_over_plain"] = ares["batched_mixed"]["solves_per_s"] / base
+    out["alkanes_631g"] = ares
+
+    dimer = geometry.water_dimer(3)
+    E0, D0 = serve.solve_parent(dimer)
+    reqs = serve.make_request_stream(count=n_requests, rate=200.0, seed=11, parent_density=D0, dimer=dimer)
+    sres = {"requests": n_requests, "rate_req_per_s": 200.0,
+            "plain_sequential": solve_plain([r.shells for r in reqs[:16]], [r.guess for r in reqs[:16]])}
+    served = {}
+    for name, mixed in (("served_fp64", False), ("served_mixed", True)):
+        sv = serve.serve(reqs, conv=1e-10, boys_mode=BOYS_REF, mixed=mixed, max_iter=64)
+        served[name] = {r.rid: (r.energy, r.status) for r in sv["results"]}
+        sres[name] = {k: v for k, v in sv.items() if k != "results"}
+    pairs = [(served["served_fp64"][k][0], v[0]) for k, v in served["served_mixed"].items()
+             if v[1] == 0 and served["served_fp64"].get(k, (0, 1))[1] == 0]
+    sres["served_mixed"]["max_abs_dE_vs_fp64"] = max(abs(a - m) for a, m in pairs) if pairs else None
+    base = sres["plain_sequential"]["solves_per_s"]
+    sres["served_fp64_over_plain"] = sres["served_fp64"]["solves_per_s"] / base
+    sres["served_mixed_over_plain"] = sres["served_mixed"]["solves_per_s"] / base
+    out["serve"] = sres
+    return out
 
 
 def main():
@@ -359,6 +463,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dss", choices=["dss", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the SCF / batch / serving measurements")
+    ap.add_argument("--forms-molecules", type=int, default=256, help="alkanes in the batched-form measurement")
+    ap.add_argument("--forms-requests", type=int, default=200, help="requests in the serving measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -61,17 +61,23 @@ class Batch:
         return h.value
 
     @staticmethod
-    def opts(conv: float = 1e-8, diis_size: int = 8, max_iter: int = 128):
-        return _lib.DssScfOpts(conv, diis_size, max_iter, 0, 0, 1e-7, 1e-12, 8, 1e-5)
+    def opts(conv: float = 1e-8, diis_size: int = 8, max_iter: int = 128, mixed: bool = False,
+             fp32_threshold: float = 1e-7, skip_threshold: float = 1e-12, rebuild_every: int = 8,
+             final_switch: float = 1e-5):
+        """SCF options; mixed=True selects the mixed-precision incremental form."""
+        return _lib.DssScfOpts(conv, diis_size, max_iter, 0, 1 if mixed else 0, fp32_threshold, skip_threshold,
+                               rebuild_every, final_switch)
 
-    def step(self, iterations: int = 1, conv: float = 1e-8, max_iter: int = 128) -> int:
-        o = self.opts(conv, max_iter=max_iter)
+    def step(self, iterations: int = 1, conv: float = 1e-8, max_iter: int = 128, mixed: bool = False,
+             fp32_threshold: float = 1e-7) -> int:
+        o = self.opts(conv, max_iter=max_iter, mixed=mixed, fp32_threshold=fp32_threshold)
         act = ctypes.c_int()
         self._check(self._L.dss_batch_step(self._h, ctypes.byref(o), iterations, ctypes.byref(act)))
         return act.value
 
-    def solve(self, conv: float = 1e-8, max_iter: int = 128) -> None:
-        o = self.opts(conv, max_iter=max_iter)
+    def solve(self, conv: float = 1e-8, max_iter: int = 128, mixed: bool = False,
+              fp32_threshold: float = 1e-7) -> None:
+        o = self.opts(conv, max_iter=max_iter, mixed=mixed, fp32_threshold=fp32_threshold)
         self._check(self._L.dss_batch_solve(self._h, ctypes.byref(o)))
 
     def result(self, handle: int, nbf: int = 0, want_density: bool = False) -> Tuple[float, Optional[np.ndarray], int, int]:

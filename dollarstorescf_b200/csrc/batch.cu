@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -33,12 +34,16 @@ namespace {
 
 // Region layout (doubles): header, then matrices of n*n each, then rings, eps.
 constexpr int kHdr = 256;
-enum Mat { M_H, M_S, M_X, M_D, M_DT, M_J, M_K, M_G, M_FN, M_F, M_T1, M_T2, M_CP, M_C, M_V, M_T3, M_NMAT };
+// M_GP, M_DP: G and D of the previous build (incremental form).
+enum Mat { M_H, M_S, M_X, M_D, M_DT, M_J, M_K, M_G, M_FN, M_F, M_T1, M_T2, M_CP, M_C, M_V, M_T3, M_GP, M_DP, M_NMAT };
 // Header slots
 constexpr int H_E = 0, H_EPREV = 1, H_TRDG = 2, H_ENUC = 3, H_DOTS = 4, H_COEF = 16, H_B = 32, H_TRDH = 140,
               H_EFINAL = 141, H_INT = 200;
-// Integer header (as int view of doubles from H_INT): iteration, done, diis count, diis slot, nocc, n, status
-constexpr int I_IT = 0, I_DONE = 1, I_CNT = 2, I_SLOT = 3, I_NOCC = 4, I_N = 5, I_STATUS = 6, I_FINAL = 7;
+// Integer header (as int view of doubles from H_INT): iteration, done, diis count, diis slot, nocc, n, status,
+// final energy present; incremental form: iteration of the last full build, full builds in a row, final
+// phase reached, the current iteration is a full build.
+constexpr int I_IT = 0, I_DONE = 1, I_CNT = 2, I_SLOT = 3, I_NOCC = 4, I_N = 5, I_STATUS = 6, I_FINAL = 7,
+              I_LASTFULL = 8, I_STREAK = 9, I_FPHASE = 10, I_FULL = 11;
 
 __host__ __device__ inline size_t region_size(int n, int ds) {
   const size_t n2 = (size_t)n * n;
@@ -80,6 +85,98 @@ __global__ void k_prep(BatchView v) {
     mat(base, n, M_DT)[t] = 2.0 * mat(base, n, M_D)[t];
     mat(base, n, M_J)[t] = 0.0;
     mat(base, n, M_K)[t] = 0.0;
+  }
+}
+
+// Incremental form: which molecules run a full build this iteration (the
+// single-molecule rule of dss_scf_solve: the first two iterations, every
+// rebuild_every-th, and all of the final phase), then Dt = 2 D (full) or
+// 2 (D - D_prev), J = K = 0.
+__global__ void k_mode(BatchView v, int rebuild_every) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb || !v.active[b]) return;
+  int* ih = ihdr(v.arena + v.region[b]);
+  const int it = ih[I_IT] + 1;
+  const int full = ih[I_FPHASE] || it <= 2 || it - ih[I_LASTFULL] >= rebuild_every;
+  ih[I_FULL] = full;
+  if (full) {
+    ih[I_LASTFULL] = it;
+    ih[I_STREAK] += 1;
+  } else {
+    ih[I_STREAK] = 0;
+  }
+}
+
+__global__ void k_force_full(BatchView v) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.nb) return;
+  int* ih = ihdr(v.arena + v.region[b]);
+  ih[I_LASTFULL] = -(1 << 30);
+  ih[I_STREAK] = 0;
+}
+
+__global__ void k_prep_inc(BatchView v) {
+  BV_BEGIN();
+  const bool full = ihdr(base)[I_FULL] != 0;
+  const double* D = mat(base, n, M_D);
+  const double* Dp = mat(base, n, M_DP);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    mat(base, n, M_DT)[t] = full ? 2.0 * D[t] : 2.0 * (D[t] - Dp[t]);
+    mat(base, n, M_J)[t] = 0.0;
+    mat(base, n, M_K)[t] = 0.0;
+  }
+}
+
+// Per shell block max |Dt| of every active molecule (the density-weighted
+// screen's bound); FLT_MAX for a full build, so that its quartets all run in FP64.
+// Shells of a molecule are consecutive in the batch basis; entry (a, b) of the
+// molecule's ns x ns block sits at sh_dbase + loc(a) ns + loc(b).
+struct BlockMaxArgs {
+  const int *sh_mol, *sh_loc, *sh_nsm, *sh_f0, *sh_nf;
+  const long long *sh_mbase, *sh_dbase;
+  float* dmax;
+  int nshell;
+};
+__global__ void k_block_max(BatchView v, BlockMaxArgs a) {
+  for (int g = blockIdx.x; g < a.nshell; g += gridDim.x) {
+    const int slot = a.sh_mol[g];
+    if (!v.active[slot]) continue;
+    const double* base = v.arena + v.region[slot];
+    const bool full = reinterpret_cast<const int*>(base + H_INT)[I_FULL] != 0;
+    const int n = v.nvec[slot], ns = a.sh_nsm[g], la = a.sh_loc[g], g0 = g - la;
+    const double* Dt = v.arena + a.sh_mbase[g];
+    const int fa = a.sh_f0[g], na = a.sh_nf[g];
+    for (int sb = threadIdx.x; sb < ns; sb += blockDim.x) {
+      float out = FLT_MAX;
+      if (!full) {
+        const int fb = a.sh_f0[g0 + sb], nbf = a.sh_nf[g0 + sb];
+        double m = 0.0;
+        for (int i = 0; i < na; ++i)
+          for (int j = 0; j < nbf; ++j) m = fmax(m, fabs(Dt[(long long)(fa + i) * n + fb + j]));
+        out = (float)(m * (1.0 + 1e-6));  // round up: the bound stays a bound in float
+      }
+      a.dmax[a.sh_dbase[g] + (long long)la * ns + sb] = out;
+    }
+  }
+}
+
+// G = (J + J^T) - (K + K^T)/2 (+ G_prev after an incremental build), F_new = H + G;
+// the incremental form keeps G and D as the next iteration's G_prev, D_prev.
+__global__ void k_fock_inc(BatchView v) {
+  BV_BEGIN();
+  const bool full = ihdr(base)[I_FULL] != 0;
+  const double* J = mat(base, n, M_J);
+  const double* K = mat(base, n, M_K);
+  double* Gp = mat(base, n, M_GP);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), c = (int)(t % n);
+    const long long u = (long long)c * n + r;
+    double g = (J[t] + J[u]) - 0.5 * (K[t] + K[u]);
+    if (!full) g += Gp[t];
+    Gp[t] = g;
+    mat(base, n, M_DP)[t] = mat(base, n, M_D)[t];
+    mat(base, n, M_G)[t] = g;
+    mat(base, n, M_FN)[t] = mat(base, n, M_H)[t] + g;
   }
 }
 
@@ -440,7 +537,10 @@ __global__ void k_trace(BatchView v, int kx, int hs) {
 
 // E_elec = 2 sum_occ eps - tr(D G); iteration count, convergence (checkConvergence),
 // iteration cap; active flags for the next iteration; counts molecules still active.
-__global__ void k_energy(BatchView v, double conv, int max_iter, int* active_out, int* n_active) {
+// Incremental form (inc != 0): convergence also needs the last two builds to have
+// been full ones, and |dE| < final_switch starts the final (all full) phase.
+__global__ void k_energy(BatchView v, double conv, int max_iter, int inc, double final_switch, int* active_out,
+                         int* n_active) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= v.nb) return;
   if (!v.active[b]) {
@@ -458,11 +558,13 @@ __global__ void k_energy(BatchView v, double conv, int max_iter, int* active_out
   base[H_E] = e;
   ih[I_IT] += 1;
   int act = 1;
+  const double de = fabs(e - base[H_EPREV]);
+  if (inc && de < final_switch) ih[I_FPHASE] = 1;
   if (!isfinite(e)) {
     ih[I_DONE] = 1;
     ih[I_STATUS] = DSS_ERR_NOCONV;
     act = 0;
-  } else if (fabs(e - base[H_EPREV]) < conv) {
+  } else if (de < conv && (!inc || ih[I_STREAK] >= 2)) {
     ih[I_DONE] = 1;
     ih[I_STATUS] = DSS_OK;
     act = 0;
@@ -546,8 +648,9 @@ struct dss_batch {
   int nmax = 0;
   int* h_nact = nullptr;  // pinned
   cudaGraphExec_t graph = nullptr;
-  double graph_conv = -1.0;
-  int graph_maxit = -1;
+  bool have_graph_opts = false;
+  dss_scf_opts graph_opts{};  // the options the captured iteration was built with
+  int inc = 0;                // the last step ran the incremental form (finalize follows it)
   ~dss_batch() {
     if (graph) cudaGraphExecDestroy(graph);
     if (h_nact) cudaFreeHost(h_nact);
@@ -656,6 +759,8 @@ int rebuild(dss_batch* b) {
   int rc = dss_setup_pairs(ctx, std::move(B));
   if (rc != DSS_OK) return bfail(b, rc, ctx->err);
   ctx->nbf = 1;  // batch mode: accumulators are addressed per molecule
+  if (ctx->d_dmax.resize((size_t)std::max<long long>(dtot, 1)) != cudaSuccess)
+    return bfail(b, DSS_ERR_OOM, "batch: device tables");
   auto up = [&](auto& buf, const auto& host) -> int {
     if (buf.resize(host.size()) != cudaSuccess) return DSS_ERR_OOM;
     if (cudaMemcpyAsync(buf.ptr, host.data(), host.size() * sizeof(host[0]), cudaMemcpyHostToDevice, ctx->stream) !=
@@ -682,21 +787,56 @@ __global__ void k_active_from_hdr(BatchView v, int* active, int want_final) {
   active[b] = want_final ? (ih[I_DONE] && !ih[I_FINAL]) : !ih[I_DONE];
 }
 
-// One SCF iteration for the active molecules (the captured body).
-int enqueue_iteration(dss_batch* b, double conv, int max_iter) {
+bool same_opts(const dss_scf_opts& a, const dss_scf_opts& c) {
+  return a.conv == c.conv && a.max_iter == c.max_iter && a.incremental == c.incremental &&
+         a.fp32_threshold == c.fp32_threshold && a.skip_threshold == c.skip_threshold &&
+         a.rebuild_every == c.rebuild_every && a.final_switch == c.final_switch;
+}
+
+// One SCF iteration for the active molecules (the captured body).  The
+// incremental form (o.incremental) follows dss_scf_solve's: G = G_prev +
+// G[2 dD] with the density-weighted screen (FP32 quartets below fp32_threshold,
+// skipped below skip_threshold), full FP64 builds per molecule at the start,
+// every rebuild_every iterations and in the final phase, accurate Boys function.
+int enqueue_iteration(dss_batch* b, const dss_scf_opts& o) {
   dss_ctx* ctx = b->ctx;
   cudaStream_t s = ctx->stream;
   const int nb = (int)b->slot_mol.size();
   BatchView v = view(b, b->d_active.ptr);
   const long long nn = (long long)b->nmax * b->nmax;
-  k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
   ctx->d_mol_active = b->d_active.ptr;
   BuildMode bm;
   bm.boys = ctx->opts.boys_mode;
   bm.no_zero = true;
+  if (o.incremental) {
+    k_mode<<<(nb + 127) / 128, 128, 0, s>>>(v, o.rebuild_every);
+    k_prep_inc<<<grid2(nn, nb), 256, 0, s>>>(v);
+    BlockMaxArgs ba;
+    ba.sh_mol = ctx->d_sh_mol.ptr;
+    ba.sh_loc = ctx->d_sh_loc.ptr;
+    ba.sh_nsm = ctx->d_sh_nsm.ptr;
+    ba.sh_f0 = ctx->d_sh_f0.ptr;
+    ba.sh_nf = ctx->d_sh_nf.ptr;
+    ba.sh_mbase = ctx->d_sh_mbase.ptr;
+    ba.sh_dbase = ctx->d_sh_dbase.ptr;
+    ba.dmax = ctx->d_dmax.ptr;
+    ba.nshell = ctx->nshell;
+    k_block_max<<<(unsigned)std::min(ctx->nshell, 4096), 64, 0, s>>>(v, ba);
+    bm.boys = DSS_BOYS_FAST;
+    bm.mixed = 1;
+    bm.dmax = ctx->d_dmax.ptr;
+    bm.fp32_thr = o.fp32_threshold;
+    bm.skip_thr = o.skip_threshold;
+  } else {
+    k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
+  }
   int rc = dss_enqueue_jk(ctx, b->arena.ptr, b->arena.ptr, b->arena.ptr, nullptr, &bm);
   if (rc != DSS_OK) return rc;
-  k_fock<<<grid2(nn, nb), 256, 0, s>>>(v);
+  if (o.incremental) {
+    k_fock_inc<<<grid2(nn, nb), 256, 0, s>>>(v);
+  } else {
+    k_fock<<<grid2(nn, nb), 256, 0, s>>>(v);
+  }
   const int tiles = (b->nmax + 31) / 32;
   const dim3 gg(tiles, tiles, nb), gb(32, 8);
   // DIIS error e = S D F_new - (S D F_new)^T
@@ -731,7 +871,8 @@ int enqueue_iteration(dss_batch* b, double conv, int max_iter) {
   // E_elec = 2 sum eps_occ - tr(D G), G from the previous density
   k_trace<<<nb, 256, 0, s>>>(v, M_G, H_TRDG);
   if (cudaMemsetAsync(b->d_nact.ptr, 0, sizeof(int), s) != cudaSuccess) return DSS_ERR_CUDA;
-  k_energy<<<(nb + 127) / 128, 128, 0, s>>>(v, conv, max_iter, b->d_active_next.ptr, b->d_nact.ptr);
+  k_energy<<<(nb + 127) / 128, 128, 0, s>>>(v, o.conv, o.max_iter, o.incremental, o.final_switch,
+                                            b->d_active_next.ptr, b->d_nact.ptr);
   if (cudaMemcpyAsync(b->d_active.ptr, b->d_active_next.ptr, nb * sizeof(int), cudaMemcpyDeviceToDevice, s) !=
       cudaSuccess)
     return DSS_ERR_CUDA;
@@ -752,7 +893,7 @@ int finalize(dss_batch* b) {
   k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
   ctx->d_mol_active = b->d_active.ptr;
   BuildMode bm;
-  bm.boys = ctx->opts.boys_mode;
+  bm.boys = b->inc ? DSS_BOYS_FAST : ctx->opts.boys_mode;  // FP64 build; the incremental form's Boys function
   bm.no_zero = true;
   int rc = dss_enqueue_jk(ctx, b->arena.ptr, b->arena.ptr, b->arena.ptr, nullptr, &bm);
   if (rc != DSS_OK) return rc;
@@ -817,7 +958,7 @@ __global__ void k_pack_d(const double* D, double* p, int n) {
   if (r <= c) p[(long long)c * (c + 1) / 2 + r] = D[t];
 }
 
-int capture_graph(dss_batch* b, double conv, int max_iter) {
+int capture_graph(dss_batch* b, const dss_scf_opts& o) {
   cudaStream_t s = b->ctx->stream;
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
@@ -826,7 +967,7 @@ int capture_graph(dss_batch* b, double conv, int max_iter) {
   cudaGraph_t g = nullptr;
   if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return bfail(b, DSS_ERR_CUDA, "batch: stream capture failed to start");
-  const int rc = enqueue_iteration(b, conv, max_iter);
+  const int rc = enqueue_iteration(b, o);
   const cudaError_t e = cudaStreamEndCapture(s, &g);
   if (rc != DSS_OK || e != cudaSuccess || !g) {
     if (g) cudaGraphDestroy(g);
@@ -836,8 +977,8 @@ int capture_graph(dss_batch* b, double conv, int max_iter) {
   const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
   cudaGraphDestroy(g);
   if (ie != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("batch: graph instantiate: ") + cudaGetErrorString(ie));
-  b->graph_conv = conv;
-  b->graph_maxit = max_iter;
+  b->graph_opts = o;
+  b->have_graph_opts = true;
   return DSS_OK;
 }
 
@@ -926,6 +1067,8 @@ int dss_batch_step(dss_batch* b, const dss_scf_opts* opts, int iterations, int* 
   dss_scf_opts o;
   dss_default_scf_opts(&o);
   if (opts) o = *opts;
+  if (o.incremental && (o.rebuild_every < 1 || !(o.fp32_threshold >= 0.0) || !(o.skip_threshold >= 0.0)))
+    return bfail(b, DSS_ERR_INVALID, "dss_batch_step: incremental form needs rebuild_every >= 1 and thresholds >= 0");
   cudaSetDevice(b->ctx->opts.device);
   cudaStream_t s = b->ctx->stream;
   bool fresh = false;
@@ -941,13 +1084,19 @@ int dss_batch_step(dss_batch* b, const dss_scf_opts* opts, int iterations, int* 
     BatchView v = view(b, b->d_active.ptr);
     k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v, b->d_active.ptr, 0);
   }
+  if ((o.incremental != 0) != (b->inc != 0)) {
+    // Switching forms: G_prev / D_prev may be stale, the next build is a full one.
+    BatchView v = view(b, b->d_active.ptr);
+    k_force_full<<<(nb + 127) / 128, 128, 0, s>>>(v);
+  }
+  b->inc = o.incremental != 0;
   int act = nb;
   for (int it = 0; it < iterations && act > 0; ++it) {
-    if (!b->graph || b->graph_conv != o.conv || b->graph_maxit != o.max_iter) {
+    if (!b->graph || !b->have_graph_opts || !same_opts(b->graph_opts, o)) {
       // First iteration after a change runs eagerly (sets kernel attributes), then capture.
-      int rc = enqueue_iteration(b, o.conv, o.max_iter);
+      int rc = enqueue_iteration(b, o);
       if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: launch failed");
-      rc = capture_graph(b, o.conv, o.max_iter);
+      rc = capture_graph(b, o);
       if (rc != DSS_OK) return rc;
     } else {
       if (cudaGraphLaunch(b->graph, s) != cudaSuccess) return bfail(b, DSS_ERR_CUDA, "dss_batch_step: graph launch");

@@ -54,7 +54,7 @@ __device__ __forceinline__ double ref_ipow(double x, unsigned p) {
 }
 
 template <int L>
-__device__ __forceinline__ void boys_ref_series(double x, double* F) {
+__device__ __noinline__ void boys_ref_series(double x, double* F) {
   const double ex = exp(-x);
   // m values with x > 1.1 m + 25 take the asymptotic branch; they are the lowest m.
   // Series for the remaining m are built from the top down.
@@ -182,9 +182,32 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
     const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
     if (!(x > thr)) m_series_lo = m;
   }
+  // The reference's asymptotic form (2m-1)!!/2^(m+1) sqrt(PI/x^(2m+1)) for the low
+  // orders, as (2m-1)!!/2^(m+1) sqrt(PI) * rsqrt(x)^(2m+1); (2m-1)!! is the
+  // reference's 32-bit value.  Same numbers to ~1e-15 relative, no loops.
+  double asym[L + 1];
+  if (m_series_lo > 0) {
+    const double y = rsqrt(x);
+    const double y2 = y * y;
+    double pw = y * 1.7724538509055152;  // sqrt(PI_REF) * x^-(1/2)
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+      unsigned int dfi = 1u;
+      for (int j = 2 * m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
+      double p2 = 1.0;
+      for (int j = 0; j < m + 1; ++j) p2 *= 2.0;
+      asym[m] = ((double)(int)dfi / p2) * pw;
+      pw *= y2;
+    }
+  }
+  if (m_series_lo > L) {
+#pragma unroll
+    for (int m = 0; m <= L; ++m) F[m] = asym[m];
+    return;
+  }
   // One code path for all lanes of a warp (their x differ): the series runs only
-  // for orders outside the tables, x ~ 0, x beyond the table, or all-asymptotic.
-  bool use_series = L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || m_series_lo > L || !(x > 1e-280) || !(x < 35.9);
+  // for orders outside the tables, x ~ 0, x beyond the table, or next to a stop.
+  bool use_series = L >= DSS_BOYS_NLB || L + 6 >= DSS_BOYS_NM || !(x > 1e-280) || !(x < 35.9);
   int n = 1;
   if (!use_series) {
     // Truncation index of the m = L series.
@@ -220,9 +243,10 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
   // most 0.37 there for every x < 36, so 20 further terms reach below 2e-18,
   // where they no longer change S (S >= 1) at double precision.  A fixed trip
   // count keeps the warp's lanes together.
+  constexpr int kTail = 20;
   double tail = 0.0, t = tn;
 #pragma unroll
-  for (int j = 1; j <= 20; ++j) {
+  for (int j = 1; j <= kTail; ++j) {
     t = t * x2 * odd_inv(L + n + j);
     tail += t;
   }
@@ -259,16 +283,8 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
     F[m] = ex * odd_inv(m) * S;
   }
 #pragma unroll
-  for (int m = 0; m <= L; ++m) {
-    if (m < m_series_lo) {
-      unsigned int dfi = 1u;
-      for (int j = 2 * m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
-      const double df = (double)(int)dfi;
-      double p2 = 1.0;
-      for (int j = 0; j < m + 1; ++j) p2 *= 2.0;
-      F[m] = df / p2 * sqrt(DSS_PI_REF / ref_ipow(x, 2 * m + 1));
-    }
-  }
+  for (int m = 0; m <= L; ++m)
+    if (m < m_series_lo) F[m] = asym[m];
 }
 
 template <int BOYS, int L>

@@ -93,10 +93,11 @@ def solve_parent(dimer, boys_mode: int = BOYS_REF, conv: float = 1e-10):
 
 def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boys_mode: int = BOYS_REF,
           arena_bytes: int = 0, iterations_per_step: int = 1, realtime: bool = True,
-          batch: Optional[Batch] = None) -> Dict:
+          batch: Optional[Batch] = None, mixed: bool = False) -> Dict:
     """Runs the request stream; returns per-request results and summary stats.
     realtime=True replays arrivals against the wall clock; False admits each
-    request as soon as it is reached in arrival order (a closed loop)."""
+    request as soon as it is reached in arrival order (a closed loop).
+    mixed=True iterates every molecule in the mixed-precision incremental form."""
     own = batch is None
     b = batch if batch is not None else Batch(schwarz_threshold=1e-12, boys_mode=boys_mode, arena_bytes=arena_bytes)
     pending = sorted(requests, key=lambda r: r.arrival)
@@ -133,7 +134,7 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
                 if qi < len(pending) and realtime:
                     time.sleep(max(0.0, pending[qi].arrival - (time.perf_counter() - t0)))
                 continue
-            b.step(iterations_per_step, conv=conv, max_iter=max_iter)
+            b.step(iterations_per_step, conv=conv, max_iter=max_iter, mixed=mixed)
             for h in list(inflight):
                 if b.finished(h):
                     E, _, it, st = b.result(h)

@@ -228,7 +228,10 @@ int dss_batch_add(dss_batch* batch, int n_shell, const int* l, const int* nprim,
 
 /* Runs up to `iterations` SCF iterations of every unfinished molecule, then
  * computes the final energies of those that finished.  *n_active: molecules
- * still iterating. */
+ * still iterating.  opts->incremental = 1 runs the mixed-precision incremental
+ * form per molecule exactly as dss_scf_solve does (full FP64 builds at the start,
+ * every rebuild_every iterations and in the final phase; FP32 / skipped quartets
+ * by the Schwarz x |dD| bound otherwise; accurate Boys function). */
 int dss_batch_step(dss_batch* batch, const dss_scf_opts* opts, int iterations, int* n_active);
 
 /* Steps until every molecule finished (converged or reached max_iter). */

@@ -61,3 +61,40 @@ def test_batch_admission_by_memory():
         with pytest.raises(Exception) as e:
             b.add(sh)
         assert "not admitted" in str(e.value)
+
+
+MIXED_SET = ["water_631gs", "dimer_631gs", "ch4_631g", "w4_631gs", "w8_631gs"]
+
+
+def test_batch_mixed_form_within_one_microhartree_and_same_alone():
+    """The incremental mixed-precision form run for a whole batch: every
+    molecule within 1 uEh of the reference's energy, and its result the same
+    when it is solved alone (its FP32/skip decisions depend on its own data only)."""
+    cases = [load_case(n) for n in MIXED_SET]
+    with Batch(schwarz_threshold=1e-12, boys_mode=BOYS_REF) as b:
+        hs = [b.add(sh) for (_, _, sh) in cases]
+        b.solve(conv=1e-10, mixed=True)
+        res = [b.result(h) for h in hs]
+    for (d, _, _), (E, _, it, st) in zip(cases, res):
+        assert st == 0
+        assert abs(E - float(d["E"])) < 1e-6, (E, float(d["E"]))
+    for (d, _, sh), (Em, _, itm, _) in zip(cases, res):
+        with Batch(schwarz_threshold=1e-12, boys_mode=BOYS_REF) as b:
+            h = b.add(sh)
+            b.solve(conv=1e-10, mixed=True)
+            Ea, _, ita, st = b.result(h)
+        assert st == 0
+        assert abs(Ea - Em) < 1e-9, (Ea, Em)
+
+
+def test_batch_switches_between_plain_and_mixed_forms():
+    """A batch that runs a few mixed iterations and then finishes in the plain
+    form ends at the plain form's energy (the switch forces a full build)."""
+    d, _, sh = load_case("w4_631gs")
+    with Batch(schwarz_threshold=1e-12, boys_mode=BOYS_REF) as b:
+        h = b.add(sh)
+        b.step(5, conv=1e-10, mixed=True)
+        b.solve(conv=1e-10)
+        E, _, it, st = b.result(h)
+    assert st == 0
+    assert abs(E - float(d["E"])) < 1e-9

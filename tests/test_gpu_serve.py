@@ -47,3 +47,25 @@ def test_warm_start_from_parent_density():
     Ec, _, itc, _ = solo_energy(sh, None)
     assert abs(Ew - Ec) < 1e-8
     assert itw < itc
+
+
+def test_served_mixed_form_equals_solo_and_within_one_microhartree():
+    """The mixed-precision incremental form served: each result equals the same
+    molecule's mixed solve alone, and lies within 1 uEh of its FP64 energy."""
+    dimer = geometry.water_dimer(3)
+    E0, D0 = serve.solve_parent(dimer)
+    reqs = serve.make_request_stream(count=16, rate=200.0, seed=5, parent_density=D0, dimer=dimer)
+    out = serve.serve(reqs, conv=1e-10, mixed=True)
+    assert out["solves"] == len(reqs)
+    assert out["peak_inflight"] > 1
+    by_id = {r.rid: r for r in out["results"]}
+    for req in reqs[:8]:
+        res = by_id[req.rid]
+        assert res.status == 0
+        with Batch(schwarz_threshold=1e-12, boys_mode=BOYS_REF) as b:
+            h = b.add(req.shells, guess=req.guess)
+            b.solve(conv=1e-10, mixed=True)
+            Em, _, _, _ = b.result(h)
+        E64, _, _, _ = solo_energy(req.shells, req.guess)
+        assert abs(res.energy - Em) < 1e-9, (req.kind, res.energy, Em)
+        assert abs(res.energy - E64) < 1e-6, (req.kind, res.energy, E64)

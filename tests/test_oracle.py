@@ -118,5 +118,5 @@ def test_reference_harness_reproduces_golden_energy():
     refpy.setup(sh)
     E, D, it, _ = refpy.scf(1e-10)
     assert E == pytest.approx(float(d["E"]), abs=1e-12)
-    # The value measured for BASELINE config 1.
+    # The reference CPU program's published energy for water / STO-3G.
     assert E == pytest.approx(-74.9629349034878, abs=1e-12)
