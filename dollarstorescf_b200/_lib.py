@@ -121,6 +121,10 @@ def load():
     L.dss_batch_solve.restype = ctypes.c_int
     L.dss_batch_result.argtypes = [vp, ctypes.c_int, dp, dp, ip, ip]
     L.dss_batch_result.restype = ctypes.c_int
+    L.dss_batch_profile.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.dss_batch_profile.restype = ctypes.c_int
+    L.dss_batch_finished.argtypes = [vp, ip, ctypes.c_int, ip]
+    L.dss_batch_finished.restype = ctypes.c_int
     L.dss_batch_remove.argtypes = [vp, ctypes.c_int]
     L.dss_batch_remove.restype = ctypes.c_int
     L.dss_batch_info.argtypes = [vp, ip, llp, llp]

@@ -3,7 +3,7 @@ together, with molecules joining and leaving between SCF iterations."""
 from __future__ import annotations
 
 import ctypes
-from typing import Optional, Tuple
+from typing import List, Optional, Tuple
 
 import numpy as np
 
@@ -89,6 +89,16 @@ class Batch:
                                              ctypes.byref(it), ctypes.byref(st)))
         return E.value, D, it.value, st.value
 
+    def finished_handles(self) -> List[int]:
+        """Handles whose results the last step produced (one library call)."""
+        cnt = ctypes.c_int()
+        self._check(self._L.dss_batch_finished(self._h, None, 0, ctypes.byref(cnt)))
+        if not cnt.value:
+            return []
+        arr = (ctypes.c_int * cnt.value)()
+        self._check(self._L.dss_batch_finished(self._h, arr, cnt.value, ctypes.byref(cnt)))
+        return list(arr)
+
     def finished(self, handle: int) -> bool:
         E = ctypes.c_double()
         return self._L.dss_batch_result(self._h, handle, ctypes.byref(E), None, None, None) == 0
@@ -102,6 +112,20 @@ class Batch:
         rb = ctypes.c_longlong(n_for_region)
         self._check(self._L.dss_batch_info(self._h, ctypes.byref(nl), ctypes.byref(fb), ctypes.byref(rb)))
         return nl.value, fb.value, rb.value if n_for_region else 0
+
+    def profile(self):
+        """Per-class milliseconds of one J/K accumulation over all live molecules."""
+        nc = self._L.dss_num_classes()
+        ms = (ctypes.c_float * nc)()
+        self._check(self._L.dss_batch_profile(self._h, ms))
+        return [float(v) for v in ms]
+
+    def work_stats(self) -> Tuple[int, int, int]:
+        """(shell quartets, primitive quartets, warp tasks) of the current composition."""
+        sq, pq, wt = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        ctx = self._L.dss_batch_context(self._h)
+        self._check(self._L.dss_work_stats(ctx, ctypes.byref(sq), ctypes.byref(pq), ctypes.byref(wt)))
+        return sq.value, pq.value, wt.value
 
     def set_class_variant(self, i: int, variant: int) -> None:
         self._check(self._L.dss_batch_set_class_variant(self._h, i, variant))

@@ -574,7 +574,7 @@ __global__ void k_energy(BatchView v, double conv, int max_iter, int inc, double
     act = 0;
   }
   active_out[b] = act;
-  if (act) atomicAdd(n_active, 1);
+  atomicAdd(n_active + (act ? 0 : 1), 1);  // [0] still iterating, [1] finished in this iteration
 }
 
 // Final energy E = 2 tr(D H) + tr(D G) + E_nuc (calculateEnergies, Energy.cpp:21-50).
@@ -630,6 +630,7 @@ struct dss_batch_mol {
   long long region = -1;
   size_t size = 0;
   BasisHost basis;  // molecule-local
+  PairSet pairs;    // its shell pairs and Schwarz factors, made once at admission
 };
 
 struct dss_batch {
@@ -646,9 +647,11 @@ struct dss_batch {
   DevBuf<long long> d_region;
   DevBuf<int> d_n, d_active, d_active_next, d_nact;
   int nmax = 0;
-  int* h_nact = nullptr;  // pinned
+  int* h_nact = nullptr;  // pinned: molecules still iterating, molecules finished in the last iteration
+  std::vector<int> last_finished;  // handles whose results the last dss_batch_step produced
   cudaGraphExec_t graph = nullptr;
   bool have_graph_opts = false;
+  bool eager_ran = false;     // an eager iteration ran since the last change (next one captures)
   dss_scf_opts graph_opts{};  // the options the captured iteration was built with
   int inc = 0;                // the last step ran the incremental form (finalize follows it)
   ~dss_batch() {
@@ -712,6 +715,7 @@ int rebuild(dss_batch* b) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+  b->eager_ran = false;
   if (!nb) {
     b->dirty = false;
     return DSS_OK;
@@ -755,8 +759,16 @@ int rebuild(dss_batch* b) {
   }
   B.nbf = 0;
   ctx->nmol = nb;
-  ctx->basis = B;
-  int rc = dss_setup_pairs(ctx, std::move(B));
+  std::vector<const PairSet*> parts(nb);
+  std::vector<int> shell_off(nb);
+  for (int s = 0, off = 0; s < nb; ++s) {
+    parts[s] = &b->mols[b->slot_mol[s]].pairs;
+    shell_off[s] = off;
+    off += (int)b->mols[b->slot_mol[s]].basis.l.size();
+  }
+  PairSet P;
+  dss_pairs_merge(parts, shell_off, &P);
+  int rc = dss_pairs_install(ctx, std::move(B), std::move(P));
   if (rc != DSS_OK) return bfail(b, rc, ctx->err);
   ctx->nbf = 1;  // batch mode: accumulators are addressed per molecule
   if (ctx->d_dmax.resize((size_t)std::max<long long>(dtot, 1)) != cudaSuccess)
@@ -774,7 +786,7 @@ int rebuild(dss_batch* b) {
       (rc = up(b->d_n, nv)))
     return bfail(b, rc, "batch: device tables");
   if (b->d_active.resize(nb) != cudaSuccess || b->d_active_next.resize(nb) != cudaSuccess ||
-      b->d_nact.resize(1) != cudaSuccess)
+      b->d_nact.resize(2) != cudaSuccess)
     return bfail(b, DSS_ERR_OOM, "batch: device tables");
   b->dirty = false;
   return DSS_OK;
@@ -870,7 +882,7 @@ int enqueue_iteration(dss_batch* b, const dss_scf_opts& o) {
   k_density<<<grid2(nn, nb), 256, 0, s>>>(v);
   // E_elec = 2 sum eps_occ - tr(D G), G from the previous density
   k_trace<<<nb, 256, 0, s>>>(v, M_G, H_TRDG);
-  if (cudaMemsetAsync(b->d_nact.ptr, 0, sizeof(int), s) != cudaSuccess) return DSS_ERR_CUDA;
+  if (cudaMemsetAsync(b->d_nact.ptr, 0, 2 * sizeof(int), s) != cudaSuccess) return DSS_ERR_CUDA;
   k_energy<<<(nb + 127) / 128, 128, 0, s>>>(v, o.conv, o.max_iter, o.incremental, o.final_switch,
                                             b->d_active_next.ptr, b->d_nact.ptr);
   if (cudaMemcpyAsync(b->d_active.ptr, b->d_active_next.ptr, nb * sizeof(int), cudaMemcpyDeviceToDevice, s) !=
@@ -888,6 +900,12 @@ int finalize(dss_batch* b) {
   if (!nb) return DSS_OK;
   BatchView v0 = view(b, b->d_active.ptr);
   k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v0, b->d_active.ptr, 1);
+  std::vector<int> fin(nb);
+  if (cudaMemcpyAsync(fin.data(), b->d_active.ptr, nb * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return DSS_ERR_CUDA;
+  for (int k = 0; k < nb; ++k)
+    if (fin[k]) b->last_finished.push_back(b->slot_mol[k]);
   BatchView v = view(b, b->d_active.ptr);
   const long long nn = (long long)b->nmax * b->nmax;
   k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
@@ -931,7 +949,7 @@ int dss_batch_create(dss_batch** out, const dss_opts* opts, size_t arena_bytes, 
     return DSS_ERR_OOM;
   }
   b->free_list.push_back({0, b->arena_doubles});
-  if (cudaMallocHost((void**)&b->h_nact, sizeof(int)) != cudaSuccess) {
+  if (cudaMallocHost((void**)&b->h_nact, 2 * sizeof(int)) != cudaSuccess) {
     delete b;
     return DSS_ERR_OOM;
   }
@@ -1013,6 +1031,9 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   rc = dss_one_electron_basis(m.basis, natom, Z, xyz, S.data(), T.data(), V.data(), &e_nuc, &err);
   if (rc != DSS_OK) return bfail(b, rc, err);
   for (size_t i = 0; i < np; ++i) T[i] += V[i];  // H
+  cudaSetDevice(b->ctx->opts.device);
+  rc = dss_pairs_make(b->ctx, m.basis, &m.pairs);
+  if (rc != DSS_OK) return bfail(b, rc, std::string("dss_batch_add: shell pairs: ") + b->ctx->err);
   m.size = region_size(m.n, b->ds);
   size_t off = 0;
   if (!arena_alloc(b, m.size, &off))
@@ -1090,24 +1111,41 @@ int dss_batch_step(dss_batch* b, const dss_scf_opts* opts, int iterations, int* 
     k_force_full<<<(nb + 127) / 128, 128, 0, s>>>(v);
   }
   b->inc = o.incremental != 0;
-  int act = nb;
+  int act = nb, newly_done = 0;
+  b->last_finished.clear();
   for (int it = 0; it < iterations && act > 0; ++it) {
-    if (!b->graph || !b->have_graph_opts || !same_opts(b->graph_opts, o)) {
-      // First iteration after a change runs eagerly (sets kernel attributes), then capture.
+    const bool graph_ok = b->graph && b->have_graph_opts && same_opts(b->graph_opts, o);
+    if (!graph_ok && !(b->eager_ran && b->have_graph_opts && same_opts(b->graph_opts, o))) {
+      // First iteration after a change of composition or options runs eagerly
+      // (it also sets kernel attributes); the graph is captured only when a
+      // second iteration follows without a change, so a serving loop whose
+      // composition changes every step does not pay for captures it never replays.
+      if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+      }
       int rc = enqueue_iteration(b, o);
       if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: launch failed");
-      rc = capture_graph(b, o);
-      if (rc != DSS_OK) return rc;
+      b->graph_opts = o;
+      b->have_graph_opts = true;
+      b->eager_ran = true;
     } else {
+      if (!graph_ok) {
+        const int rc = capture_graph(b, o);
+        if (rc != DSS_OK) return rc;
+      }
       if (cudaGraphLaunch(b->graph, s) != cudaSuccess) return bfail(b, DSS_ERR_CUDA, "dss_batch_step: graph launch");
     }
-    cudaMemcpyAsync(b->h_nact, b->d_nact.ptr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(b->h_nact, b->d_nact.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
     const cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_step: ") + cudaGetErrorString(e));
-    act = *b->h_nact;
+    act = b->h_nact[0];
+    newly_done += b->h_nact[1];
   }
-  const int rc = finalize(b);
-  if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: final energies");
+  if (newly_done > 0) {  // final energies only when some molecule finished
+    const int rc = finalize(b);
+    if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: final energies");
+  }
   // Restore the iteration flags for the next step.
   BatchView v = view(b, b->d_active.ptr);
   k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v, b->d_active.ptr, 0);
@@ -1159,6 +1197,7 @@ int dss_batch_remove(dss_batch* b, int handle) {
   arena_free(b, (size_t)m.region, m.size);
   m.live = false;
   m.basis = BasisHost();
+  m.pairs = PairSet();
   b->dirty = true;
   return DSS_OK;
 }
@@ -1186,7 +1225,57 @@ int dss_batch_set_class_variant(dss_batch* b, int i, int variant) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+  b->eager_ran = false;
   return rc;
+}
+
+int dss_batch_profile(dss_batch* b, float* ms) {
+  if (!b || !ms) return DSS_ERR_INVALID;
+  b->err.clear();
+  const int ncls = dss_num_classes();
+  for (int i = 0; i < ncls; ++i) ms[i] = 0.0f;
+  cudaSetDevice(b->ctx->opts.device);
+  if (b->dirty) {
+    const int rc = rebuild(b);
+    if (rc != DSS_OK) return rc;
+  }
+  const int nb = (int)b->slot_mol.size();
+  if (!nb) return DSS_OK;
+  dss_ctx* ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  // Every live molecule takes part (J and K are scratch: the next iteration rebuilds them).
+  DevBuf<int> all;
+  if (all.resize(nb) != cudaSuccess) return bfail(b, DSS_ERR_OOM, "dss_batch_profile: allocation");
+  std::vector<int> ones(nb, 1);
+  cudaMemcpyAsync(all.ptr, ones.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s);
+  BatchView v = view(b, all.ptr);
+  const long long nn = (long long)b->nmax * b->nmax;
+  k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
+  ctx->d_mol_active = all.ptr;
+  const int nc = (int)ctx->tasks.size();
+  std::vector<cudaEvent_t> ev(2 * nc);
+  for (auto& e : ev) cudaEventCreate(&e);
+  BuildMode bm;
+  bm.boys = ctx->opts.boys_mode;
+  bm.no_zero = true;
+  int rc = dss_enqueue_jk(ctx, b->arena.ptr, b->arena.ptr, b->arena.ptr, ev.data(), &bm);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (rc == DSS_OK && e == cudaSuccess)
+    for (int i = 0; i < nc && i < ncls; ++i)
+      if (ctx->tasks[i].ntasks) cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+  for (auto& x : ev) cudaEventDestroy(x);
+  ctx->d_mol_active = b->d_active.ptr;
+  if (rc != DSS_OK) return bfail(b, rc, "dss_batch_profile: launch failed");
+  if (e != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_profile: ") + cudaGetErrorString(e));
+  return DSS_OK;
+}
+
+int dss_batch_finished(const dss_batch* b, int* handles, int cap, int* count) {
+  if (!b || !count || (cap > 0 && !handles)) return DSS_ERR_INVALID;
+  const int n = (int)b->last_finished.size();
+  for (int i = 0; i < n && i < cap; ++i) handles[i] = b->last_finished[i];
+  *count = n;
+  return DSS_OK;
 }
 
 void* dss_batch_context(dss_batch* b) { return b ? (void*)b->ctx : nullptr; }

@@ -239,11 +239,12 @@ __device__ __forceinline__ void boys_ref(double x, double* F) {
   const double ex = exp(-x);
   const double x2 = 2.0 * x;
   const double tn = exp((double)n * log(x2) - g_boys_lp[L * (DSS_BOYS_NB + 1) + n]);
-  // Tail beyond the stop: t_n <= 1e-9 and the term ratio 2x/(2L+2n+2j+1) is at
-  // most 0.37 there for every x < 36, so 20 further terms reach below 2e-18,
-  // where they no longer change S (S >= 1) at double precision.  A fixed trip
-  // count keeps the warp's lanes together.
-  constexpr int kTail = 20;
+  // Tail beyond the stop: t_n <= 1e-9 and the term ratio 2x/(2L+2n+2j+1) stays
+  // below 0.37 there; scanning x in (0, 1.1 L + 25] shows that what is left
+  // after 8 + floor(L/2) further terms is below 1e-17 S (L <= 8), so 10 + L/2 terms
+  // leave S unchanged at double precision (orders above 8, not scanned, keep 20).
+  // A fixed trip count keeps the warp's lanes together.
+  constexpr int kTail = L <= 8 ? 10 + L / 2 : 20;
   double tail = 0.0, t = tn;
 #pragma unroll
   for (int j = 1; j <= kTail; ++j) {

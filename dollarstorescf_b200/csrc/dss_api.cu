@@ -314,18 +314,21 @@ int dss_build_jk(dss_ctx* ctx, const double* Dp, double* Jp, double* Kp) {
 }  // extern "C"
 
 // ------------------------------------------------------------------ pairs, Schwarz, tasks
-int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
+static_assert(sizeof(PrimPair) == 10 * sizeof(double), "PairSet stores primitive pairs as 10 doubles");
+
+int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out) {
   const int ns = (int)B.l.size();
-  // Unordered shell pairs {a, b}; stored with l_a >= l_b (ties: a >= b).
+  // Unordered shell pairs {a, b} inside one molecule; stored with l_a >= l_b (ties: a >= b).
   struct PairTmp {
     int a, b, cls, npp, mol;
   };
   const bool batch = !B.mol.empty();
   std::vector<PairTmp> pairs;
-  pairs.reserve((size_t)ns * (ns + 1) / 2);
-  for (int i = 0; i < ns; ++i)
-    for (int j = 0; j <= i; ++j) {
-      if (batch && B.mol[i] != B.mol[j]) continue;  // pairs only inside a molecule
+  pairs.reserve((size_t)ns * 8);
+  int first = 0;  // first shell of the current molecule (shells of a molecule are consecutive)
+  for (int i = 0; i < ns; ++i) {
+    if (batch && i > 0 && B.mol[i] != B.mol[i - 1]) first = i;
+    for (int j = first; j <= i; ++j) {
       int a = i, b = j;
       if (B.l[j] > B.l[i]) std::swap(a, b);
       // Primitive pairs kept by the primitive screen (same test as below).
@@ -338,6 +341,7 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
           if (keep_prim_pair(B, a, p, b, q, ab2, ctx->opts.primitive_threshold)) ++kept;
       pairs.push_back({a, b, pair_class_index(B.l[a], B.l[b]), kept, batch ? B.mol[a] : 0});
     }
+  }
   // Order by class, molecule, then primitive-pair count (descending), then original order.
   std::stable_sort(pairs.begin(), pairs.end(), [](const PairTmp& x, const PairTmp& y) {
     if (x.cls != y.cls) return x.cls < y.cls;
@@ -376,51 +380,42 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
         pp.push_back(r);
       }
   }
-  ctx->release_basis();
-  ctx->nbf = B.nbf;
-  ctx->pure = B.pure;
-  ctx->nshell = ns;
+  // Schwarz factors on the device (scratch buffers), one launch per pair class.
+  DevBuf<PrimPair> d_pp;
+  DevBuf<int> d_pa, d_pb, d_p0, d_pn;
+  DevBuf<double> d_xyz, d_Q;
   int rc;
-  if ((rc = upload(ctx, ctx->d_pp, pp)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_a, pa)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_b, pb)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_pp0, p0)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_npp, pn)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_sh_xyz, B.xyz)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_sh_f0, B.f0)) != DSS_OK) return rc;
-  DSS_CUDA(ctx->d_Q.resize(np));
-
-  // Class ranges.
-  const int ncls = DSS_N_PAIR_CLASSES;
-  std::vector<int> c0(ncls, 0), c1(ncls, 0);
-  for (int c = 0, q = 0; c < ncls; ++c) {
-    c0[c] = q;
-    while (q < np && pairs[q].cls == c) ++q;
-    c1[c] = q;
-  }
-  // Schwarz factors on the device, one launch per pair class.
-  for (int la = 0; la <= DSS_GEN_LMAX; ++la)
+  if ((rc = upload(ctx, d_pp, pp)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, d_pa, pa)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, d_pb, pb)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, d_p0, p0)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, d_pn, pn)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, d_xyz, B.xyz)) != DSS_OK) return rc;
+  DSS_CUDA(d_Q.resize(std::max(np, 1)));
+  for (int la = 0, q = 0; la <= DSS_GEN_LMAX; ++la)
     for (int lb = 0; lb <= la; ++lb) {
       const int c = pair_class_index(la, lb);
-      if (c1[c] == c0[c]) continue;
+      const int q0 = q;
+      while (q < np && pairs[q].cls == c) ++q;
+      if (q == q0) continue;
       SchwarzArgs sa;
-      sa.pair0 = c0[c];
-      sa.npair = c1[c] - c0[c];
-      sa.pair_a = ctx->d_pair_a.ptr;
-      sa.pair_b = ctx->d_pair_b.ptr;
-      sa.pair_pp0 = ctx->d_pair_pp0.ptr;
-      sa.pair_npp = ctx->d_pair_npp.ptr;
-      sa.pp = ctx->d_pp.ptr;
-      sa.sh_xyz = ctx->d_sh_xyz.ptr;
-      sa.Q = ctx->d_Q.ptr;
-      dss_launch_schwarz(la, lb, ctx->opts.boys_mode, ctx->pure, sa, ctx->stream);
+      sa.pair0 = q0;
+      sa.npair = q - q0;
+      sa.pair_a = d_pa.ptr;
+      sa.pair_b = d_pb.ptr;
+      sa.pair_pp0 = d_p0.ptr;
+      sa.pair_npp = d_pn.ptr;
+      sa.pp = d_pp.ptr;
+      sa.sh_xyz = d_xyz.ptr;
+      sa.Q = d_Q.ptr;
+      dss_launch_schwarz(la, lb, ctx->opts.boys_mode, B.pure, sa, ctx->stream);
       DSS_CUDA(cudaGetLastError());
     }
   std::vector<double> Q(np);
-  DSS_CUDA(cudaMemcpyAsync(Q.data(), ctx->d_Q.ptr, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (np) DSS_CUDA(cudaMemcpyAsync(Q.data(), d_Q.ptr, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   DSS_CUDA(cudaStreamSynchronize(ctx->stream));
 
-  // Within each (class, npp) group: Schwarz factor descending.
+  // Within each (class, molecule, npp) group: Schwarz factor descending.
   std::vector<int> perm(np);
   for (int q = 0; q < np; ++q) perm[q] = q;
   std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) {
@@ -429,38 +424,118 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
     if (pairs[x].npp != pairs[y].npp) return pairs[x].npp > pairs[y].npp;
     return Q[x] > Q[y];
   });
-  std::vector<int> pa2(np), pb2(np), p02(np), pn2(np), cls2(np), mol2(np);
-  std::vector<double> Q2(np);
+  PairSet& P = *out;
+  P = PairSet();
+  P.pa.resize(np);
+  P.pb.resize(np);
+  P.p0.resize(np);
+  P.pn.resize(np);
+  P.cls.resize(np);
+  P.mol.resize(np);
+  P.Q.resize(np);
   for (int q = 0; q < np; ++q) {
     const int o = perm[q];
-    pa2[q] = pa[o];
-    pb2[q] = pb[o];
-    p02[q] = p0[o];
-    pn2[q] = pn[o];
-    cls2[q] = pairs[o].cls;
-    mol2[q] = pairs[o].mol;
-    Q2[q] = Q[o];
+    P.pa[q] = pa[o];
+    P.pb[q] = pb[o];
+    P.p0[q] = p0[o];
+    P.pn[q] = pn[o];
+    P.cls[q] = pairs[o].cls;
+    P.mol[q] = pairs[o].mol;
+    P.Q[q] = Q[o];
   }
-  if ((rc = upload(ctx, ctx->d_pair_a, pa2)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_b, pb2)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_pp0, p02)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_pair_npp, pn2)) != DSS_OK) return rc;
-  if ((rc = upload(ctx, ctx->d_Qs, Q2)) != DSS_OK) return rc;
+  P.pp.resize(pp.size() * 10);
+  if (!pp.empty()) std::memcpy(P.pp.data(), pp.data(), pp.size() * sizeof(PrimPair));
+  return DSS_OK;
+}
+
+void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out) {
+  PairSet& P = *out;
+  P = PairSet();
+  size_t np = 0, npp = 0;
+  for (const PairSet* s : parts) {
+    np += s->pa.size();
+    npp += s->pp.size();
+  }
+  P.pa.reserve(np);
+  P.pb.reserve(np);
+  P.p0.reserve(np);
+  P.pn.reserve(np);
+  P.cls.reserve(np);
+  P.mol.reserve(np);
+  P.Q.reserve(np);
+  P.pp.reserve(npp);
+  std::vector<int> pp_off(parts.size()), cur(parts.size(), 0);
+  for (size_t m = 0; m < parts.size(); ++m) {
+    pp_off[m] = (int)(P.pp.size() / 10);
+    P.pp.insert(P.pp.end(), parts[m]->pp.begin(), parts[m]->pp.end());
+  }
+  // Each part is sorted by class first: walking the classes in order and taking
+  // every part's run of that class gives the (class, molecule, ...) order.
+  for (int c = 0; c < DSS_N_PAIR_CLASSES; ++c)
+    for (size_t m = 0; m < parts.size(); ++m) {
+      const PairSet& s = *parts[m];
+      int& q = cur[m];
+      for (; q < (int)s.pa.size() && s.cls[q] == c; ++q) {
+        P.pa.push_back(s.pa[q] + shell_offset[m]);
+        P.pb.push_back(s.pb[q] + shell_offset[m]);
+        P.p0.push_back(s.p0[q] + pp_off[m]);
+        P.pn.push_back(s.pn[q]);
+        P.cls.push_back(c);
+        P.mol.push_back((int)m);
+        P.Q.push_back(s.Q[q]);
+      }
+    }
+}
+
+int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P) {
+  const int np = (int)P.pa.size();
+  ctx->nbf = B.nbf;
+  ctx->pure = B.pure;
+  ctx->nshell = (int)B.l.size();
+  int rc;
+  // Device buffers are reused when large enough (grow-only), so a batch whose
+  // composition changes does not free and reallocate them every time.
+  DSS_CUDA(ctx->d_pp.resize(std::max<size_t>(P.pp.size() / 10, 1)));
+  if (!P.pp.empty())
+    DSS_CUDA(cudaMemcpyAsync(ctx->d_pp.ptr, P.pp.data(), P.pp.size() * sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  if ((rc = upload(ctx, ctx->d_pair_a, P.pa)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_b, P.pb)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_pp0, P.p0)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_pair_npp, P.pn)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_Qs, P.Q)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_sh_xyz, B.xyz)) != DSS_OK) return rc;
+  if ((rc = upload(ctx, ctx->d_sh_f0, B.f0)) != DSS_OK) return rc;
   {
     std::vector<int> nf(ctx->nshell);
-    for (int q = 0; q < ctx->nshell; ++q) nf[q] = ctx->basis.pure ? 2 * ctx->basis.l[q] + 1
-                                                                  : (ctx->basis.l[q] + 1) * (ctx->basis.l[q] + 2) / 2;
+    for (int q = 0; q < ctx->nshell; ++q) nf[q] = B.pure ? 2 * B.l[q] + 1 : (B.l[q] + 1) * (B.l[q] + 2) / 2;
     if ((rc = upload(ctx, ctx->d_sh_nf, nf)) != DSS_OK) return rc;
   }
-  ctx->h_pair_a = pa2;
-  ctx->h_pair_b = pb2;
-  ctx->h_pair_npp = pn2;
-  ctx->h_pair_cls = cls2;
-  ctx->h_pair_mol = mol2;
-  ctx->h_Q = Q2;
+  // Class ranges.
+  const int ncls = DSS_N_PAIR_CLASSES;
+  std::vector<int> c0(ncls, 0), c1(ncls, 0);
+  for (int c = 0, q = 0; c < ncls; ++c) {
+    c0[c] = q;
+    while (q < np && P.cls[q] == c) ++q;
+    c1[c] = q;
+  }
+  ctx->h_pair_a = std::move(P.pa);
+  ctx->h_pair_b = std::move(P.pb);
+  ctx->h_pair_npp = std::move(P.pn);
+  ctx->h_pair_cls = std::move(P.cls);
+  ctx->h_pair_mol = std::move(P.mol);
+  ctx->h_Q = std::move(P.Q);
   ctx->class_pair0 = c0;
   ctx->class_pair1 = c1;
+  ctx->basis = std::move(B);
   return dss_build_tasks(ctx);
+}
+
+int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
+  PairSet P;
+  int rc = dss_pairs_make(ctx, B, &P);
+  if (rc != DSS_OK) return rc;
+  return dss_pairs_install(ctx, std::move(B), std::move(P));
 }
 
 int dss_build_tasks(dss_ctx* ctx) {
@@ -490,6 +565,8 @@ int dss_build_tasks(dss_ctx* ctx) {
       q = e;
     }
   }
+  // The previous work-list buffers are reused (grow-only) by the new lists.
+  std::vector<ClassTasks> old = std::move(ctx->tasks);
   ctx->tasks.clear();
   ctx->n_shell_quartets = 0;
   ctx->n_prim_quartets = 0;
@@ -505,6 +582,7 @@ int dss_build_tasks(dss_ctx* ctx) {
   for (const ClassInfo& ci : kClasses) {
     const int bc = ci.bc, kc = ci.kc;
     ClassTasks ct;
+    if (ctx->tasks.size() < old.size()) ct.d_tasks = std::move(old[ctx->tasks.size()].d_tasks);
     ct.la = ci.la;
     ct.lb = ci.lb;
     ct.lc = ci.lc;

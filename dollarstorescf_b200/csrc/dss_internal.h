@@ -150,6 +150,20 @@ struct dss_ctx {
 
 int dss_fail(dss_ctx* ctx, int code, const std::string& msg);
 int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what);
+// Shell pairs of a basis with their primitive pairs and Schwarz factors, sorted
+// by (pair class, molecule, primitive-pair count descending, Q descending).
+struct PairSet {
+  std::vector<int> pa, pb, p0, pn, cls, mol;  // shells, first primitive pair, primitive pairs, class, molecule
+  std::vector<double> Q;
+  std::vector<double> pp;  // primitive pairs, 10 doubles each (the PrimPair record)
+};
+// Pairs of one basis (Schwarz factors computed on the device, synchronously).
+int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out);
+// Concatenation of per-molecule pair sets in batch order: part m's shells start
+// at shell_offset[m] and its pairs become molecule m's.
+void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out);
+// Makes B and P the context's basis: uploads, class ranges, work lists.
+int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P);
 int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
 // Shells from the C-ABI arrays: validation and the reference's primitive normalisation.
 int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,

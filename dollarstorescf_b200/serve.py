@@ -135,12 +135,13 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
                     time.sleep(max(0.0, pending[qi].arrival - (time.perf_counter() - t0)))
                 continue
             b.step(iterations_per_step, conv=conv, max_iter=max_iter, mixed=mixed)
-            for h in list(inflight):
-                if b.finished(h):
-                    E, _, it, st = b.result(h)
-                    r, adm = inflight.pop(h)
-                    b.remove(h)
-                    results.append(Result(r.rid, r.kind, E, it, st, r.arrival, adm, time.perf_counter() - t0))
+            for h in b.finished_handles():
+                if h not in inflight:
+                    continue
+                E, _, it, st = b.result(h)
+                r, adm = inflight.pop(h)
+                b.remove(h)
+                results.append(Result(r.rid, r.kind, E, it, st, r.arrival, adm, time.perf_counter() - t0))
     finally:
         if own:
             b.close()

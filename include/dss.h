@@ -242,6 +242,17 @@ int dss_batch_solve(dss_batch* batch, const dss_scf_opts* opts);
 int dss_batch_result(dss_batch* batch, int handle, double* E_total, double* D_packed, int* iterations,
                      int* status);
 
+/* Handles of the molecules whose results the last dss_batch_step produced
+ * (converged or stopped in it); *count is their number, at most cap are written.
+ * One call replaces polling dss_batch_result per molecule. */
+int dss_batch_finished(const dss_batch* batch, int* handles, int cap, int* count);
+
+/* One J/K accumulation over every live molecule's current density with CUDA
+ * events around each class launch (classes one after another on one stream):
+ * ms[i] = milliseconds of class i in dss_class_info order, 0 for classes without
+ * work.  Overwrites the molecules' J/K scratch only; for the batch autotuner. */
+int dss_batch_profile(dss_batch* batch, float* ms);
+
 /* Releases a molecule's region. */
 int dss_batch_remove(dss_batch* batch, int handle);
 
