@@ -314,11 +314,14 @@ def run_gpu(args):
     achieved = fl[dom]["flops"] / dom_t / 1e12 if dom_t > 0 else 0.0
     total_flops = sum(c["flops"] for c in fl)
     sq, pq, wt = fb.work_stats()
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    traffic = None  # DRAM bytes per launch of the dominant kernel, from the committed ncu capture
+    tpath = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.isfile(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("eri_jk_kernel_%s" % fl[dom]["class"])
+            for ln in f:
+                p = ln.split()
+                if len(p) == 2 and not ln.startswith("#") and p[0] == "eri_jk_kernel<%s>" % fl[dom]["class"]:
+                    traffic = int(p[1])
     kern = fb.kernels_per_build()
 
     line = {
