@@ -370,129 +370,43 @@ __global__ void k_diis_combine(BatchView v) {
   }
 }
 
-__device__ __forceinline__ void rr_pair(int m, int r, int k, int& p, int& q) {
-  if (k == 0) {
-    p = m - 1;
-    q = r;
-  } else {
-    p = (r + k) % (m - 1);
-    q = (r - k + (m - 1)) % (m - 1);
-  }
-  if (p > q) {
-    const int t = p;
-    p = q;
-    q = t;
-  }
-}
-
 // Cyclic Jacobi, one block per molecule: A (matrix ka, overwritten) -> eigenvalues
-// ascending in eps, eigenvectors as columns of matrix kv (via the spare kt).
-template <bool SMEM>
-__global__ void __launch_bounds__(256) k_jacobi(BatchView v, int ka, int kv, int kt, int max_sweeps, double tol) {
+// ascending in eps, eigenvectors as columns of matrix kv (rotations accumulate in
+// the spare matrix kt, transposed).  MODE 0: A (packed upper triangle) and VT in
+// shared memory; 1: packed A in shared memory, VT in global memory; 2: both dense
+// in global memory.  A launch takes the molecules with n_lo < n <= n_hi.
+template <int MODE>
+__global__ void __launch_bounds__(512) k_jacobi(BatchView v, int ka, int kv, int kt, int max_sweeps, double tol,
+                                                int n_lo, int n_hi) {
   const int b = blockIdx.x;
   if (b >= v.nb || !v.active[b]) return;
   const int n = v.nvec[b];
+  if (n <= n_lo || n > n_hi) return;
   double* base = v.arena + v.region[b];
   extern __shared__ double sm[];
-  const int m = (n % 2) ? n + 1 : n;
-  const int half = m / 2;
-  double* A = SMEM ? sm : mat(base, n, ka);
-  double* cs = SMEM ? sm + (size_t)n * n : sm;
-  double* V = mat(base, n, kv);
+  const size_t nn = (size_t)n * n, np = dss_packed_size(n);
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (SMEM)
-    for (int t = tid; t < n * n; t += nt) A[t] = mat(base, n, ka)[t];
-  for (int t = tid; t < n * n; t += nt) V[t] = (t / n == t % n) ? 1.0 : 0.0;
-  __shared__ double red[2][8];
-  __syncthreads();
-  for (int sweep = 0; sweep <= max_sweeps; ++sweep) {
-    double off = 0.0, dia = 0.0;
-    for (int t = tid; t < n * n; t += nt) {
-      const double x = A[t];
-      if (t / n == t % n) dia += x * x;
-      else off += x * x;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      off += __shfl_xor_sync(0xffffffffu, off, o);
-      dia += __shfl_xor_sync(0xffffffffu, dia, o);
-    }
-    if ((tid & 31) == 0) {
-      red[0][tid >> 5] = off;
-      red[1][tid >> 5] = dia;
-    }
+  double* src = mat(base, n, ka);
+  if (MODE <= 1) {
+    double* VT = MODE == 0 ? sm + np : mat(base, n, kt);
+    void* aux = sm + np + (MODE == 0 ? nn : 0);
+    DssPackedSym A{sm, n};
+    for (int i = tid >> 5; i < n; i += nt >> 5)
+      for (int jj = i + (tid & 31); jj < n; jj += 32) A.at(i, jj) = src[(size_t)i * n + jj];
+    for (int t = tid; t < (int)nn; t += nt) VT[t] = (t / n == t % n) ? 1.0 : 0.0;
     __syncthreads();
-    double so = 0.0, sd = 0.0;
-    for (int k = 0; k < (nt >> 5); ++k) {
-      so += red[0][k];
-      sd += red[1][k];
-    }
+    dss_block_jacobi(A, VT, aux, max_sweeps, tol);
     __syncthreads();
-    if (so <= tol * tol * (so + sd) || sweep == max_sweeps) break;
-    for (int r = 0; r < m - 1; ++r) {
-      for (int k = tid; k < half; k += nt) {
-        int p, q;
-        rr_pair(m, r, k, p, q);
-        double c = 1.0, s = 0.0;
-        if (q < n) {
-          const double apq = A[p * n + q];
-          if (fabs(apq) > 1e-300) {
-            const double app = A[p * n + p], aqq = A[q * n + q];
-            const double tau = (aqq - app) / (2.0 * apq);
-            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            c = 1.0 / sqrt(1.0 + t * t);
-            s = t * c;
-          }
-        }
-        cs[k] = c;
-        cs[half + k] = s;
-      }
-      __syncthreads();
-      for (int t = tid; t < half * half; t += nt) {
-        const int k1 = t / half, k2 = t % half;
-        int p1, q1, p2, q2;
-        rr_pair(m, r, k1, p1, q1);
-        rr_pair(m, r, k2, p2, q2);
-        const double c1 = cs[k1], s1 = cs[half + k1], c2 = cs[k2], s2 = cs[half + k2];
-        const bool q1v = q1 < n, q2v = q2 < n;
-        const double b00 = A[p1 * n + p2];
-        const double b01 = q2v ? A[p1 * n + q2] : 0.0;
-        const double b10 = q1v ? A[q1 * n + p2] : 0.0;
-        const double b11 = (q1v && q2v) ? A[q1 * n + q2] : 0.0;
-        const double x00 = c1 * b00 - s1 * b10, x01 = c1 * b01 - s1 * b11;
-        const double x10 = s1 * b00 + c1 * b10, x11 = s1 * b01 + c1 * b11;
-        A[p1 * n + p2] = x00 * c2 - x01 * s2;
-        if (q2v) A[p1 * n + q2] = x00 * s2 + x01 * c2;
-        if (q1v) A[q1 * n + p2] = x10 * c2 - x11 * s2;
-        if (q1v && q2v) A[q1 * n + q2] = x10 * s2 + x11 * c2;
-      }
-      for (int t = tid; t < n * half; t += nt) {
-        const int i = t / half, k = t % half;
-        int p, q;
-        rr_pair(m, r, k, p, q);
-        if (q >= n) continue;
-        const double c = cs[k], s = cs[half + k];
-        const double vp = V[(size_t)i * n + p], vq = V[(size_t)i * n + q];
-        V[(size_t)i * n + p] = c * vp - s * vq;
-        V[(size_t)i * n + q] = s * vp + c * vq;
-      }
-      __syncthreads();
-    }
+    dss_block_jacobi_sorted(A, VT, eps_of(base, n, v.ds), mat(base, n, kv));
+  } else {
+    double* VT = mat(base, n, kt);
+    DssDenseSym A{src, n};
+    for (int t = tid; t < (int)nn; t += nt) VT[t] = (t / n == t % n) ? 1.0 : 0.0;
+    __syncthreads();
+    dss_block_jacobi(A, VT, sm, max_sweeps, tol);
+    __syncthreads();
+    dss_block_jacobi_sorted(A, VT, eps_of(base, n, v.ds), mat(base, n, kv));
   }
-  // Ascending eigenvalues, vectors permuted alike (through the spare matrix).
-  double* w = eps_of(base, n, v.ds);
-  double* T = mat(base, n, kt);
-  for (int i = tid; i < n; i += nt) {
-    const double wi = A[i * n + i];
-    int rk = 0;
-    for (int j = 0; j < n; ++j) {
-      const double wj = A[j * n + j];
-      if (wj < wi || (wj == wi && j < i)) ++rk;
-    }
-    w[rk] = wi;
-    for (int r2 = 0; r2 < n; ++r2) T[(size_t)r2 * n + rk] = V[(size_t)r2 * n + i];
-  }
-  __syncthreads();
-  for (int t = tid; t < n * n; t += nt) V[t] = T[t];
 }
 
 __global__ void k_copy(BatchView v, int ksrc, int kdst) {
@@ -864,17 +778,36 @@ int enqueue_iteration(dss_batch* b, const dss_scf_opts& o) {
   k_gemm<<<gg, gb, 0, s>>>(v, M_X, M_T1, M_T2, 0, 0, 1.0, 0.0);
   k_gemm<<<gg, gb, 0, s>>>(v, M_T2, M_CP, M_T1, 0, 0, 1.0, 0.0);
   k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_T1, M_T2, 1, 0, 1.0, 0.0);
-  const size_t smem_full = (size_t)b->nmax * b->nmax * 8 + (size_t)(b->nmax + 2) * 8;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_jacobi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
+  // Eigensolver, one block of 512 threads per molecule, in up to three launches
+  // by size: matrix and rotations in shared memory, matrix only, neither.
+  static int optin = 0;
+  if (!optin) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(k_jacobi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(k_jacobi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   }
-  if (smem_full <= 200 * 1024) {
-    k_jacobi<true><<<nb, 256, smem_full, s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL);
-  } else {
-    k_jacobi<false><<<nb, 256, (size_t)(b->nmax + 2) * 8, s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL);
+  auto fits = [&](int nn_, bool vt) {
+    return (dss_packed_size(nn_) + (vt ? (size_t)nn_ * nn_ : 0)) * 8 + dss_block_jacobi_smem(nn_) <= (size_t)optin;
+  };
+  int n1 = 0, n2 = 0;
+  while (fits(n1 + 1, true)) ++n1;
+  while (fits(n2 + 1, false)) ++n2;
+  int top[3] = {0, 0, 0};
+  for (int k = 0; k < nb; ++k) {
+    const int nk = b->mols[b->slot_mol[k]].n;
+    const int mode = nk <= n1 ? 0 : (nk <= n2 ? 1 : 2);
+    top[mode] = std::max(top[mode], nk);
   }
+  if (top[0])
+    k_jacobi<0><<<nb, 512, (dss_packed_size(top[0]) + (size_t)top[0] * top[0]) * 8 + dss_block_jacobi_smem(top[0]),
+                  s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL, 0, n1);
+  if (top[1])
+    k_jacobi<1><<<nb, 512, dss_packed_size(top[1]) * 8 + dss_block_jacobi_smem(top[1]), s>>>(
+        v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL, n1, n2);
+  if (top[2])
+    k_jacobi<2><<<nb, 512, dss_block_jacobi_smem(top[2]), s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL, n2, 1 << 30);
   // C' <- C' V (through T1), C = X C', D = C_occ C_occ^T
   k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_V, M_T1, 0, 0, 1.0, 0.0);
   k_copy<<<grid2(nn, nb), 256, 0, s>>>(v, M_T1, M_CP);

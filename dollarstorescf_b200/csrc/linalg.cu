@@ -48,22 +48,6 @@ __global__ void gemm_kernel(int n, bool ta, bool tb, double alpha, const double*
   }
 }
 
-// Round-robin (circle method) pairing for m players: round r, slot k.
-__device__ __forceinline__ void rr_pair(int m, int r, int k, int& p, int& q) {
-  if (k == 0) {
-    p = m - 1;
-    q = r;
-  } else {
-    p = (r + k) % (m - 1);
-    q = (r - k + (m - 1)) % (m - 1);
-  }
-  if (p > q) {
-    const int t = p;
-    p = q;
-    q = t;
-  }
-}
-
 __global__ void __launch_bounds__(256) jacobi_kernel(int n, int m, double* A0, double* A1, double* V0, double* V1,
                                                      double* w, double* scratch, int* rank, int max_sweeps,
                                                      double tol) {
@@ -79,6 +63,7 @@ __global__ void __launch_bounds__(256) jacobi_kernel(int n, int m, double* A0, d
   double* Vc = V0;
   double* Vn = V1;
   __shared__ double red[2][8];
+  double off_prev = 0.0;
   for (int sweep = 0; sweep <= max_sweeps; ++sweep) {
     // Off-diagonal and total Frobenius norms (slots alternate between sweeps).
     double* slot = scratch + 2 * (sweep & 1);
@@ -116,11 +101,12 @@ __global__ void __launch_bounds__(256) jacobi_kernel(int n, int m, double* A0, d
     grid.sync();
     const double offv = slot[0], tot = slot[0] + slot[1];
     if (gtid == 0) scratch[4] = (double)sweep;
-    if (offv <= tol * tol * tot || sweep == max_sweeps) break;
+    if (dss_jacobi_done(offv, tot, off_prev, sweep, max_sweeps, tol)) break;
+    off_prev = offv;
     for (int r = 0; r < m - 1; ++r) {
       for (int k = threadIdx.x; k < half; k += blockDim.x) {
         int p, q;
-        rr_pair(m, r, k, p, q);
+        dss_rr_pair(m, r, k, p, q);
         double c = 1.0, s = 0.0;
         if (q < n) {
           const double apq = A[(size_t)p * n + q];
@@ -140,8 +126,8 @@ __global__ void __launch_bounds__(256) jacobi_kernel(int n, int m, double* A0, d
       for (long long t = gtid; t < (long long)half * half; t += gsz) {
         const int k1 = (int)(t / half), k2 = (int)(t % half);
         int p1, q1, p2, q2;
-        rr_pair(m, r, k1, p1, q1);
-        rr_pair(m, r, k2, p2, q2);
+        dss_rr_pair(m, r, k1, p1, q1);
+        dss_rr_pair(m, r, k2, p2, q2);
         const double c1 = cs_c[k1], s1 = cs_s[k1], c2 = cs_c[k2], s2 = cs_s[k2];
         const bool q1v = q1 < n, q2v = q2 < n;
         const double b00 = A[(size_t)p1 * n + p2];
@@ -161,7 +147,7 @@ __global__ void __launch_bounds__(256) jacobi_kernel(int n, int m, double* A0, d
       for (long long t = gtid; t < (long long)n * half; t += gsz) {
         const int i = (int)(t / half), k = (int)(t % half);
         int p, q;
-        rr_pair(m, r, k, p, q);
+        dss_rr_pair(m, r, k, p, q);
         const double c = cs_c[k], s = cs_s[k];
         const double vp = Vc[(size_t)i * n + p];
         if (q < n) {
@@ -203,6 +189,30 @@ __global__ void __launch_bounds__(256) jacobi_kernel(int n, int m, double* A0, d
     for (long long t = gtid; t < (long long)n * n; t += gsz) V0[t] = Vn[t];
 }
 
+// One thread block for a matrix that fits in shared memory as a packed upper
+// triangle (no grid-wide synchronisation between the rounds); VT_SMEM: the
+// rotations in shared memory too, else in VTg.
+template <bool VT_SMEM>
+__global__ void __launch_bounds__(512) jacobi_block_kernel(int n, const double* A0, double* V, double* w, double* VTg,
+                                                            int max_sweeps, double tol, int v_init) {
+  extern __shared__ double sm[];
+  const size_t nn = (size_t)n * n, np = dss_packed_size(n);
+  DssPackedSym A{sm, n};
+  double* VT = VT_SMEM ? sm + np : VTg;
+  void* aux = sm + np + (VT_SMEM ? nn : 0);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid >> 5; i < n; i += nt >> 5)
+    for (int j = i + (tid & 31); j < n; j += 32) A.at(i, j) = A0[(size_t)i * n + j];
+  for (int t = tid; t < (int)nn; t += nt) {
+    const int i = t / n, j = t % n;
+    VT[t] = v_init ? V[(size_t)j * n + i] : (i == j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  dss_block_jacobi(A, VT, aux, max_sweeps, tol);
+  __syncthreads();
+  dss_block_jacobi_sorted(A, VT, w, V);
+}
+
 __global__ void set_identity(int n, double* V) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < (long long)n * n) V[t] = (t / n == t % n) ? 1.0 : 0.0;
@@ -219,6 +229,25 @@ void dss_gemm(cudaStream_t s, int n, bool ta, bool tb, double alpha, const doubl
 
 cudaError_t dss_jacobi_eigh(cudaStream_t s, int n, double* A, double* V, double* w, double* work, int max_sweeps,
                             double tol, bool v_init) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int optin[64] = {};
+  if (dev >= 0 && dev < 64 && !optin[dev]) {
+    cudaDeviceGetAttribute(&optin[dev], cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(jacobi_block_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin[dev]);
+    cudaFuncSetAttribute(jacobi_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin[dev]);
+  }
+  const size_t one = dss_packed_size(n) * 8 + dss_block_jacobi_smem(n), two = one + (size_t)n * n * 8;
+  if (dev >= 0 && dev < 64 && two <= (size_t)optin[dev]) {
+    // Small matrices: one block, matrix and rotations in shared memory.
+    jacobi_block_kernel<true><<<1, 512, two, s>>>(n, A, V, w, work, max_sweeps, tol, v_init ? 1 : 0);
+    return cudaGetLastError();
+  }
+  if (dev >= 0 && dev < 64 && one <= (size_t)optin[dev]) {
+    // Medium: the matrix in shared memory, the rotations in work.
+    jacobi_block_kernel<false><<<1, 512, one, s>>>(n, A, V, w, work, max_sweeps, tol, v_init ? 1 : 0);
+    return cudaGetLastError();
+  }
   const int m = (n % 2) ? n + 1 : n;
   double* A1 = work;
   double* V1 = work + (size_t)n * n;
@@ -229,8 +258,6 @@ cudaError_t dss_jacobi_eigh(cudaStream_t s, int n, double* A, double* V, double*
   }
   cudaError_t e = cudaMemsetAsync(scratch, 0, 8 * sizeof(double), s);
   if (e != cudaSuccess) return e;
-  int dev = 0;
-  cudaGetDevice(&dev);
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int threads = 256;
