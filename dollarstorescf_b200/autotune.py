@@ -61,3 +61,39 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
     return choice
+
+
+def tune_batch(batch, repeats: int = 2) -> Dict[str, int]:
+    """The same per-class choice for a dss_batch: times both variants of every
+    class with work over all live molecules (dss_batch_profile) and keeps the
+    faster one.  Returns {class name: variant}."""
+    nc = batch._L.dss_num_classes()
+    timings: Dict[int, Dict[int, float]] = {}
+    for variant in (0, 1):
+        ok = []
+        for i in range(nc):
+            try:
+                batch.set_class_variant(i, variant)
+                ok.append(i)
+            except Exception:
+                pass
+        best = [math.inf] * nc
+        for _ in range(repeats):
+            ms = batch.profile()
+            for i in ok:
+                best[i] = min(best[i], ms[i])
+        for i in ok:
+            if best[i] > 0:
+                timings.setdefault(i, {})[variant] = best[i]
+    choice = {}
+    ctx = batch._L.dss_batch_context(batch._h)
+    import ctypes
+
+    for i, t in timings.items():
+        v = min(t, key=t.get)
+        batch.set_class_variant(i, v)
+        l4 = (ctypes.c_int * 4)()
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        batch._L.dss_class_info(ctx, i, l4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        choice["%d%d%d%d" % tuple(l4)] = v
+    return choice

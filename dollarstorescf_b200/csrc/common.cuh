@@ -46,7 +46,8 @@ __device__ __forceinline__ void prim_quartet(const PrimPair& b, const PrimPair& 
                                              double& rho_p, double& rho_q) {
   const double p = b.p, q = k.p;
   const double pq = p + q;
-  const double inv_pq = 1.0 / pq;
+  const double r_pq = rsqrt(pq);  // 1/sqrt(p+q); its square is 1/(p+q) to ~2 ulp
+  const double inv_pq = r_pq * r_pq;
   const double PQx = b.Px - k.Px, PQy = b.Py - k.Py, PQz = b.Pz - k.Pz;
   const double rho = p * q * inv_pq;
   const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
@@ -59,7 +60,7 @@ __device__ __forceinline__ void prim_quartet(const PrimPair& b, const PrimPair& 
   oo2p = 0.5 * b.inv_p;
   oo2q = 0.5 * k.inv_p;
   oo2pq = 0.5 * inv_pq;
-  const double pref = DSS_TWO_PI_25 * b.K * k.K * b.inv_p * k.inv_p * (inv_pq * sqrt(pq));
+  const double pref = DSS_TWO_PI_25 * b.K * k.K * b.inv_p * k.inv_p * r_pq;
   boys_eval<BOYS, L>(T, F);
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;

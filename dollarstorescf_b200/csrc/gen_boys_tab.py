@@ -71,7 +71,7 @@ def main() -> None:
         # (g_boys_rr: G_{m,n} at B_m[n]; g_boys_rl: G_{m,n} at B_m[n-1]).  A point x of I_n
         # takes the grid node k = round(16 x) when that node lies in I_n, else the
         # end of I_n on the node's side, so |x - x0| <= 1/32 always.
-        NLR, NBR = 9, 86
+        NLR, NBR = 3, 86
         mpmath.mp.dps = 30
         def taylor(m, n, x0):
             x0 = mpmath.mpf(x0)

@@ -98,3 +98,29 @@ def test_batch_switches_between_plain_and_mixed_forms():
         E, _, it, st = b.result(h)
     assert st == 0
     assert abs(E - float(d["E"])) < 1e-9
+
+
+def test_batch_finished_poll_profile_and_tuner():
+    """dss_batch_finished reports every molecule exactly once, in the step that
+    produced its result; dss_batch_profile times the classes; the batch tuner's
+    choice leaves the energies at the reference's."""
+    from dollarstorescf_b200.autotune import tune_batch
+
+    names = ["water_631gs", "dimer_631gs", "ch4_631g", "w4_631gs"]
+    cases = [load_case(n) for n in names]
+    with Batch(schwarz_threshold=1e-12, boys_mode=BOYS_REF) as b:
+        hs = [b.add(sh) for (_, _, sh) in cases]
+        ms = b.profile()
+        assert sum(ms) > 0 and min(ms) >= 0
+        assert tune_batch(b)
+        seen = []
+        for _ in range(200):
+            b.step(1, conv=1e-10)
+            seen += b.finished_handles()
+            if len(seen) >= len(hs):
+                break
+        assert sorted(seen) == sorted(hs)
+        for h, (d, _, _) in zip(hs, cases):
+            E, _, it, st = b.result(h)
+            assert st == 0
+            assert abs(E - float(d["E"])) < 1e-9
