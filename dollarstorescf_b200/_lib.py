@@ -103,6 +103,9 @@ def load():
     L.dss_scf_solve.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(DssScfOpts), dp, dp,
                                 ip]
     L.dss_scf_solve.restype = ctypes.c_int
+    L.dss_uhf_solve.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(DssScfOpts),
+                                dp, dp, dp, ip]
+    L.dss_uhf_solve.restype = ctypes.c_int
     L.dss_build_jk_device_noalloc.argtypes = [vp, vp, vp, vp]
     L.dss_build_jk_device_noalloc.restype = ctypes.c_int
     szt = ctypes.c_size_t

@@ -1,10 +1,13 @@
 """Builds libdss.so (the C-ABI engine) in-tree for sm_100a.
 
-Steps: generate the per-class ERI code (csrc/gen_eri.py) and the Boys table
+Steps: generate the per-class ERI code (csrc/gen_eri.py) and the Boys tables
 (csrc/gen_boys_tab.py) into _build/gen/, write one translation unit per
 shell-quartet class plus a dispatch unit, compile them in parallel with nvcc
 (-gencode arch=compute_100a,code=sm_100a -lineinfo -O3), and link
-dollarstorescf_b200/libdss.so with the CUDA runtime linked statically.
+dollarstorescf_b200/libdss.so with the CUDA runtime linked statically.  The
+large Boys cell table is defined once (boys_cell_data.cu) and reaches the
+kernels as a pointer; whole-program compilation keeps the kernels free of
+call-ABI spills that relocatable device code adds.
 
 Usage: python -m dollarstorescf_b200.build [--lmax 2] [--jobs N]
 """
@@ -145,15 +148,16 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     os.makedirs(obj_dir, exist_ok=True)
     eri_gen = os.path.join(GEN, "eri_gen.cuh")
     boys_tab = os.path.join(GEN, "boys_tab.cuh")
+    boys_data = os.path.join(GEN, "boys_cell_data.cu")
     gen_stamp = os.path.join(GEN, "stamp")
     want = _stamp([os.path.join(CSRC, "gen_eri.py"), os.path.join(CSRC, "gen_boys_tab.py"),
                    os.path.join(CSRC, "gen_coop.py")], str(lmax))
     have = open(gen_stamp).read() if os.path.isfile(gen_stamp) else ""
     sph_tab = os.path.join(GEN, "sph_tab.h")
     coop_gen = os.path.join(GEN, "coop_gen.cuh")
-    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, sph_tab, coop_gen)):
+    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, boys_data, sph_tab, coop_gen)):
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_eri.py"), eri_gen, str(lmax)])
-        subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_boys_tab.py"), boys_tab])
+        subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_boys_tab.py"), boys_tab, boys_data])
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_coop.py"), coop_gen, str(lmax)])
         with open(gen_stamp, "w") as f:
             f.write(want)
@@ -166,6 +170,7 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     p = os.path.join(GEN, "eri_dispatch.cu")
     _write_if_changed(p, _dispatch_tu(classes, pcls, coop))
     units.append(p)
+    units.append(boys_data)
     for name in sorted(os.listdir(CSRC)):
         if name.endswith(".cu"):
             units.append(os.path.join(CSRC, name))

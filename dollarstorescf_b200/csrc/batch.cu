@@ -959,11 +959,7 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   m.natom = natom;
   if (m.nocc > m.n) return bfail(b, DSS_ERR_INVALID, "dss_batch_add: more occupied orbitals than functions");
   const size_t np = (size_t)m.n * (m.n + 1) / 2;
-  std::vector<double> S(np), T(np), V(np);
-  double e_nuc = 0.0;
-  rc = dss_one_electron_basis(m.basis, natom, Z, xyz, S.data(), T.data(), V.data(), &e_nuc, &err);
-  if (rc != DSS_OK) return bfail(b, rc, err);
-  for (size_t i = 0; i < np; ++i) T[i] += V[i];  // H
+  const double e_nuc = dss_nuclear_repulsion(natom, Z, xyz);
   cudaSetDevice(b->ctx->opts.device);
   rc = dss_pairs_make(b->ctx, m.basis, &m.pairs);
   if (rc != DSS_OK) return bfail(b, rc, std::string("dss_batch_add: shell pairs: ") + b->ctx->err);
@@ -986,8 +982,12 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   double* dD = dS + np;
   double* work = dD + np;  // 3 n^2 + 64 + n
   double* w = work + 3 * n2 + 64 + n;
-  cudaMemcpyAsync(dH, T.data(), np * 8, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(dS, S.data(), np * 8, cudaMemcpyHostToDevice, s);
+  // S and H = T + V straight into the scratch (device one-electron kernels).
+  rc = dss_one_electron_device(s, m.basis, natom, Z, xyz, dS, dH, nullptr, &err);
+  if (rc != DSS_OK) {
+    arena_free(b, off, m.size);
+    return bfail(b, rc, err);
+  }
   if (D_guess) cudaMemcpyAsync(dD, D_guess, np * 8, cudaMemcpyHostToDevice, s);
   double* base = b->arena.ptr + off;
   k_admit_init<<<(unsigned)std::min<size_t>((n2 + 255) / 256, 1024), 256, 0, s>>>(base, n, dH, dS,

@@ -11,8 +11,10 @@
 // 2x/(2m+3) plus a leading 1, so the top m runs the full series and each lower m
 // only adjusts its truncation point by a few terms (the stopping rule is applied
 // to the m-series' own terms, exactly as the reference applies it).  The series
-// itself only runs next to a truncation breakpoint; elsewhere the values come
-// from per-interval Taylor tables (boys_ref_tab).
+// itself only runs next to a truncation breakpoint and near x = 0; elsewhere
+// the values come from per-cell Taylor records (boys_ref_cells) or, beyond
+// their orders, from the accurate function corrected by the truncated tail
+// (boys_ref_walk).
 //
 // DSS_BOYS_FAST is the accurate function: a 7-term Taylor expansion of F_L
 // about the nearest point of a 1/16-spaced table (boys_tab.cuh), downward
@@ -56,7 +58,7 @@ __device__ __forceinline__ double ref_ipow(double x, unsigned p) {
 }
 
 template <int L>
-__device__ __noinline__ void boys_ref_series(double x, double* F) {
+static __device__ __noinline__ void boys_ref_series(double x, double* F) {
   const double ex = exp(-x);
   // m values with x > 1.1 m + 25 take the asymptotic branch; they are the lowest m.
   // Series for the remaining m are built from the top down.
@@ -290,99 +292,84 @@ __device__ __forceinline__ void boys_ref_walk(double x, double* F) {
     if (m < m_series_lo) F[m] = asym[m];
 }
 
-// The reference's asymptotic form (2m-1)!!/2^(m+1) sqrt(PI/x^(2m+1)) for the
-// orders m < m_lo, as (2m-1)!!/2^(m+1) sqrt(PI) * rsqrt(x)^(2m+1); (2m-1)!! is the
-// reference's 32-bit value.  Same numbers to ~1e-15 relative, no loops.
+// Reference-mode Boys from the cell records (cells = the library's copy of
+// g_boys_cell, boys_cell_data.cu, passed in the kernel arguments): one
+// record per order m and grid point k = round(16 x) holds the Taylor
+// coefficients, about k/16, of the reference's value on both sides of the one
+// truncation breakpoint b the cell may contain (b = 1e300 when it has none).
+// The asymptotic form is evaluated for every lane (one rsqrt); a lane reads the
+// record of order m only when x <= 1.1 m + 25, picks the half by x > b and
+// evaluates it: no search, two dependent loads, seven FMAs per order.  The
+// series itself (a separate function) runs only for x < 1/32 (cell 0 holds
+// several breakpoints) and within 4e-14 (relative) of a breakpoint, where the
+// rounding of the reference's own sum decides its stop.
 template <int L>
-__device__ __forceinline__ void boys_ref_asym(double x, int m_lo, double* F) {
-  const double y = rsqrt(x);
-  const double y2 = y * y;
-  double pw = y * 1.7724538509055152;  // sqrt(PI_REF) * x^-(1/2)
+__device__ __forceinline__ void boys_ref_cells(double x, double* F, const double* __restrict__ cells) {
+  static_assert(L < DSS_BOYS_NMC, "cell records too narrow for this order");
+  // Orders m < m_lo take the asymptotic form (x > 1.1 m + 25; the thresholds
+  // grow with m, so these are the lowest orders).
+  int m_lo = L + 1;
+#pragma unroll
+  for (int m = L; m >= 0; --m)
+    if (!(x > __dadd_rn(__dmul_rn((double)m, 1.1), 25.0))) m_lo = m;
+  if (m_lo > 0) {
+    // (2m-1)!!/2^(m+1) sqrt(PI) x^-(m+1/2), (2m-1)!! as the reference's 32-bit int.
+    const double y = rsqrt(x);
+    const double y2 = y * y;
+    double pw = y * 1.7724538509055152;  // sqrt(PI_REF) * x^-(1/2)
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+      unsigned int dfi = 1u;
+      for (int j = 2 * m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
+      double p2 = 1.0;
+      for (int j = 0; j < m + 1; ++j) p2 *= 2.0;
+      if (m < m_lo) F[m] = ((double)(int)dfi / p2) * pw;
+      pw *= y2;
+    }
+  }
+  if (m_lo > L) return;
+  const int k = max(0, min(__double2int_rn(x * (double)DSS_BOYS_STEP), DSS_BOYS_NCELL - 1));
+  const double dx = x - (double)k * (1.0 / DSS_BOYS_STEP);
+  bool series = !(x >= 1.0 / 32.0);
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
-    unsigned int dfi = 1u;
-    for (int j = 2 * m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
-    double p2 = 1.0;
-    for (int j = 0; j < m + 1; ++j) p2 *= 2.0;
-    if (m < m_lo) F[m] = ((double)(int)dfi / p2) * pw;
-    pw *= y2;
+    if (m < m_lo) continue;
+    const double2* r = reinterpret_cast<const double2*>(cells) + ((size_t)m * DSS_BOYS_NCELL + k) * 8;
+    const double b = __ldg(&r[3].y);
+    const double2* c = r + (x > b ? 4 : 0);
+    const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c6b = __ldg(c + 3);
+    double f = c6b.x;
+    f = f * dx + c45.y;
+    f = f * dx + c45.x;
+    f = f * dx + c23.y;
+    f = f * dx + c23.x;
+    f = f * dx + c01.y;
+    f = f * dx + c01.x;
+    F[m] = f;
+    series = series || fabs(x - b) <= 4e-14 * x;
   }
+  if (series) boys_ref_series<L>(x, F);
 }
 
-// One order of the reference's series value from the interval tables
-// (boys_tab.cuh): inside an interval I_n = (B_m[n-1], B_m[n]] between two
-// truncation breakpoints the reference returns the analytic function
-// G_{m,n}(x) = exp(-x) sum_{i<=n} a_i x^i, so a 7-term Taylor expansion about a
-// node of the same interval (the nearest 1/16 grid point when it lies in I_n,
-// else the end of I_n on its side; |x - x0| <= 1/32) gives it to ~1e-15.
-// Returns false within 4e-14 (relative) of a breakpoint, where the rounding of
-// the reference's own sum decides the stop and the series has to run.
-__device__ __forceinline__ bool boys_ref_tab(int m, double x, double& F) {
-  const double* bp = g_boys_bp + m * (DSS_BOYS_NB + 1);
-  int n = 1 + (int)g_boys_idx[m * DSS_BOYS_NG + (int)(x * 4.0)];
-  while (n <= DSS_BOYS_NB && bp[n] < x) ++n;  // x in (bp[n-1], bp[n]]
-  if (n >= DSS_BOYS_NBR) return false;
-  const double lo = bp[n - 1], hi = bp[n];
-  if (fabs(x - hi) <= 4e-14 * x || fabs(x - lo) <= 4e-14 * x) return false;
-  const int k = __double2int_rn(x * (double)DSS_BOYS_STEP);
-  const double xk = (double)k * (1.0 / DSS_BOYS_STEP);
-  const double* c;
-  double x0;
-  if ((int)g_boys_rn[m * DSS_BOYS_NGRID + k] == n) {
-    c = g_boys_rg + ((size_t)m * DSS_BOYS_NGRID + k) * 8;
-    x0 = xk;
-  } else if (xk > hi) {
-    c = g_boys_rr + (m * DSS_BOYS_NBR + n) * 8;
-    x0 = hi;
-  } else {
-    c = g_boys_rl + (m * DSS_BOYS_NBR + n) * 8;
-    x0 = lo;
-  }
-  const double2* c2 = reinterpret_cast<const double2*>(c);
-  const double2 c01 = c2[0], c23 = c2[1], c45 = c2[2], c67 = c2[3];
-  const double dx = x - x0;
-  double f = c67.x;
-  f = f * dx + c45.y;
-  f = f * dx + c45.x;
-  f = f * dx + c23.y;
-  f = f * dx + c23.x;
-  f = f * dx + c01.y;
-  f = f * dx + c01.x;
-  F = f;
-  return true;
-}
+#ifndef DSS_BOYS_CELL_LMAX
+#define DSS_BOYS_CELL_LMAX 8
+#endif
 
-// Reference-mode Boys (the reference's flo::boysFunctionExact values): the
-// asymptotic form for the orders with x > 1.1 m + 25, the interval tables for
-// the others, the series itself next to a breakpoint and at x = 0.  From L = 3
-// on, one table lookup per order costs more than boys_ref_walk's single
-// accurate F_L plus the walk down the orders (measured on (H2O)16 6-31G*), so
-// the tables serve L <= 2.
+// Reference-mode Boys (the reference's flo::boysFunctionExact values): the cell
+// records for L <= DSS_BOYS_CELL_LMAX, boys_ref_walk above.
 template <int L>
-__device__ __forceinline__ void boys_ref(double x, double* F) {
-  if constexpr (L >= DSS_BOYS_NLR || L > 2) {
-    boys_ref_walk<L>(x, F);
+__device__ __forceinline__ void boys_ref(double x, double* F, const double* __restrict__ cells) {
+  if constexpr (L <= DSS_BOYS_CELL_LMAX && L < DSS_BOYS_NMC) {
+    boys_ref_cells<L>(x, F, cells);
   } else {
-    int m_lo = L + 1;  // orders m >= m_lo use the series value
-#pragma unroll
-    for (int m = L; m >= 0; --m) {
-      const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
-      if (!(x > thr)) m_lo = m;
-    }
-    if (m_lo > 0) boys_ref_asym<L>(x, m_lo, F);
-    if (m_lo > L) return;
-    bool ok = x > 1e-280;
-#pragma unroll
-    for (int m = 0; m <= L; ++m)
-      if (m >= m_lo && ok) ok = boys_ref_tab(m, x, F[m]);
-    if (!ok) boys_ref_series<L>(x, F);
+    boys_ref_walk<L>(x, F);
   }
 }
 
 template <int BOYS, int L>
-__device__ __forceinline__ void boys_eval(double x, double* F) {
+__device__ __forceinline__ void boys_eval(double x, double* F, const double* __restrict__ cells) {
   if constexpr (BOYS == DSS_BOYS_REF) {
-    boys_ref<L>(x, F);
+    boys_ref<L>(x, F, cells);
   } else {
     boys_fast<L>(x, F);
   }

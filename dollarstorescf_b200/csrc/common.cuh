@@ -35,7 +35,8 @@ __device__ __forceinline__ PrimPair load_pp(const PrimPair* __restrict__ src) {
 // the ERI prefactor of chem/GaussianIntegral.cpp:632.
 #define DSS_TWO_PI_25 34.98683665524963
 
-// Primitive-quartet set-up: Boys values scaled by the prefactor
+// Primitive-quartet set-up (cells: the reference-mode Boys records, see
+// boys_ref_cells): Boys values scaled by the prefactor
 //   2 pi^2.5 / (p q sqrt(p+q)) K_ab K_cd F_m(T),  T = rho |P-Q|^2,
 // and the Obara-Saika coefficients used by the vertical recursion.
 template <int BOYS, int L>
@@ -43,7 +44,7 @@ __device__ __forceinline__ void prim_quartet(const PrimPair& b, const PrimPair& 
                                              double& PAy, double& PAz, double& WPx, double& WPy, double& WPz,
                                              double& QCx, double& QCy, double& QCz, double& WQx, double& WQy,
                                              double& WQz, double& oo2p, double& oo2q, double& oo2pq,
-                                             double& rho_p, double& rho_q) {
+                                             double& rho_p, double& rho_q, const double* __restrict__ cells) {
   const double p = b.p, q = k.p;
   const double pq = p + q;
   const double r_pq = rsqrt(pq);  // 1/sqrt(p+q); its square is 1/(p+q) to ~2 ulp
@@ -61,7 +62,7 @@ __device__ __forceinline__ void prim_quartet(const PrimPair& b, const PrimPair& 
   oo2q = 0.5 * k.inv_p;
   oo2pq = 0.5 * inv_pq;
   const double pref = DSS_TWO_PI_25 * b.K * k.K * b.inv_p * k.inv_p * r_pq;
-  boys_eval<BOYS, L>(T, F);
+  boys_eval<BOYS, L>(T, F, cells);
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;
 }

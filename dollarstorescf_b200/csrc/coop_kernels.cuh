@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
         double F[L + 1];
         double* r = recs + lane * DSS_REC;
         prim_quartet<BOYS, L>(bp, kp, F, r[12], r[13], r[14], r[15], r[16], r[17], r[18], r[19], r[20], r[21],
-                              r[22], r[23], r[24], r[25], r[26], r[27], r[28]);
+                              r[22], r[23], r[24], r[25], r[26], r[27], r[28], a.boys_cell);
 #pragma unroll
         for (int m = 0; m <= L; ++m) r[m] = F[m];
       }

@@ -187,6 +187,7 @@ int dss_create(dss_ctx** out, const dss_opts* opts) {
     return DSS_ERR_INVALID;
   }
   e = cudaSetDevice(ctx->opts.device);
+  if (e == cudaSuccess) e = dss_boys_cell_table(&ctx->boys_cell);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
   for (int i = 0; i < dss_ctx::kSideStreams && e == cudaSuccess; ++i) {
     e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
@@ -408,6 +409,7 @@ int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out) {
       sa.pp = d_pp.ptr;
       sa.sh_xyz = d_xyz.ptr;
       sa.Q = d_Q.ptr;
+      sa.boys_cell = ctx->boys_cell;
       dss_launch_schwarz(la, lb, ctx->opts.boys_mode, B.pure, sa, ctx->stream);
       DSS_CUDA(cudaGetLastError());
     }
@@ -691,6 +693,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.ns = ctx->nshell;
     a.skip_thr = mode->skip_thr;
     a.fp32_thr = mode->fp32_thr;
+    a.boys_cell = ctx->boys_cell;
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], st));
     dss_launch_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, mode->mixed ? DSS_BOYS_FAST : mode->boys, ctx->pure,
                            mode->mixed, ct.variant, a, st);
@@ -882,11 +885,11 @@ int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops) {
 #include "boys.cuh"
 namespace {
 template <int L>
-__global__ void boys_check_kernel(int mode, const double* x, int n, double* F) {
+__global__ void boys_check_kernel(int mode, const double* x, int n, double* F, const double* cells) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double f[L + 1];
-  if (mode == DSS_BOYS_REF) boys_ref<L>(x[i], f);
+  if (mode == DSS_BOYS_REF) boys_ref<L>(x[i], f, cells);
   else if (mode == DSS_BOYS_FAST) boys_fast<L>(x[i], f);
   else boys_ref_series<L>(x[i], f);
   for (int m = 0; m <= L; ++m) F[(size_t)i * (L + 1) + m] = f[m];
@@ -905,7 +908,7 @@ extern "C" int dss_eval_boys(dss_ctx* ctx, int mode, int L, const double* x, int
     switch (L) {
 #define DSS_BC(l)                                                                    \
   case l:                                                                            \
-    boys_check_kernel<l><<<blocks, 128, 0, ctx->stream>>>(mode, dx.ptr, n, dF.ptr); \
+    boys_check_kernel<l><<<blocks, 128, 0, ctx->stream>>>(mode, dx.ptr, n, dF.ptr, ctx->boys_cell); \
     break;
       DSS_BC(0) DSS_BC(1) DSS_BC(2) DSS_BC(3) DSS_BC(4) DSS_BC(5) DSS_BC(6) DSS_BC(7) DSS_BC(8) DSS_BC(9)
       DSS_BC(10) DSS_BC(11) DSS_BC(12)

@@ -75,6 +75,7 @@ struct ScfBuffers {
 
 struct dss_ctx {
   dss_opts opts{};
+  const double* boys_cell = nullptr;  // device address of the Boys cell records on opts.device
   cudaStream_t stream = nullptr;      // the stream work is enqueued on
   cudaStream_t own_stream = nullptr;  // created with the context
   // Side streams: the class launches of one build fork onto them so that the
@@ -149,6 +150,9 @@ struct dss_ctx {
 };
 
 int dss_fail(dss_ctx* ctx, int code, const std::string& msg);
+// Device address of the reference-mode Boys cell records on the current device
+// (defined once in the generated boys_cell_data.cu).
+cudaError_t dss_boys_cell_table(const double** out);
 int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what);
 // Shell pairs of a basis with their primitive pairs and Schwarz factors, sorted
 // by (pair class, molecule, primitive-pair count descending, Q descending).
@@ -168,9 +172,16 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
 // Shells from the C-ABI arrays: validation and the reference's primitive normalisation.
 int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,
                    const double* centers, int pure, BasisHost* out, std::string* err);
-// One-electron S, T, V (packed-U) and nuclear repulsion of one molecule's basis.
-int dss_one_electron_basis(const BasisHost& B, int natom, const int* Z, const double* xyz, double* S, double* T,
-                           double* V, double* e_nuc, std::string* err);
+// One-electron S, T, V (packed-U, device buffers) of one molecule's basis,
+// computed on the device on stream s (synchronous).  V == NULL: T receives
+// T + V, the core Hamiltonian.
+int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz,
+                            double* S, double* T, double* V, std::string* err);
+// The same into host packed-U arrays (any may be NULL), plus the nuclear repulsion.
+int dss_one_electron_basis(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz,
+                           double* S, double* T, double* V, double* e_nuc, std::string* err);
+// sum_{A<B} Z_A Z_B / R_AB.
+double dss_nuclear_repulsion(int natom, const int* Z, const double* xyz);
 int dss_build_tasks(dss_ctx* ctx);
 // G = (Jacc + Jacc^T) - (Kacc + Kacc^T) / 2, dense n x n.
 void dss_symmetrize_combine(cudaStream_t s, int n, const double* Jacc, const double* Kacc, double* G);

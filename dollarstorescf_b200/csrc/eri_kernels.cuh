@@ -57,6 +57,7 @@ struct EriArgs {
   const long long* sh_dbase;
   const int* sh_nsm;
   const int* mol_active;
+  const double* boys_cell;  // reference-mode Boys records (dss_boys_cell_table)
 };
 
 struct SchwarzArgs {
@@ -68,6 +69,7 @@ struct SchwarzArgs {
   const PrimPair* pp;
   const double* sh_xyz;
   double* Q;              // out: sqrt(max |(ij|ij)|) per pair
+  const double* boys_cell;  // reference-mode Boys records (dss_boys_cell_table)
 };
 
 __host__ __device__ constexpr int dss_ncart(int l) { return (l + 1) * (l + 2) / 2; }
@@ -82,14 +84,14 @@ struct EriClass;
     template <int BOYS, bool PURE, typename R>                                                          \
     __device__ __forceinline__ static void evalr(const PrimPair* bra, int nb, const PrimPair* ket, int nk, \
                                                  double ABx, double ABy, double ABz, double CDx,        \
-                                                 double CDy, double CDz, R* I) {                        \
-      eri_##la##lb##lc##ld<BOYS, PURE, R>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I);          \
+                                                 double CDy, double CDz, R* I, const double* cells) {   \
+      eri_##la##lb##lc##ld<BOYS, PURE, R>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I, cells);   \
     }                                                                                                   \
     template <int BOYS, bool PURE>                                                                      \
     __device__ __forceinline__ static void eval(const PrimPair* bra, int nb, const PrimPair* ket, int nk, \
                                                 double ABx, double ABy, double ABz, double CDx,         \
-                                                double CDy, double CDz, double* I) {                    \
-      eri_##la##lb##lc##ld<BOYS, PURE, double>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I);     \
+                                                double CDy, double CDz, double* I, const double* cells) { \
+      eri_##la##lb##lc##ld<BOYS, PURE, double>(bra, nb, ket, nk, ABx, ABy, ABz, CDx, CDy, CDz, I, cells); \
     }                                                                                                   \
   };
 DSS_FOR_EACH_CLASS(DSS_DEFINE_ERI_CLASS)
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
       float If[NA * NB * NC * ND];
       EriClass<LA, LB, LC, LD>::template evalr<BOYS, PURE, float>(
           a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
-          __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, If);
+          __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, If, a.boys_cell);
 #pragma unroll
       for (int q = 0; q < NA * NB * NC * ND; ++q) I[q] = (double)If[q];
       done = true;
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
   } else if (active) {
     EriClass<LA, LB, LC, LD>::template eval<BOYS, PURE>(
         a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
-        __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, I);
+        __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, I, a.boys_cell);
   } else {
 #pragma unroll
     for (int q = 0; q < NA * NB * NC * ND; ++q) I[q] = 0.0;
@@ -291,7 +293,8 @@ __global__ void __launch_bounds__(128) schwarz_kernel(SchwarzArgs a) {
   const PrimPair* pp = a.pp + a.pair_pp0[pr];
   const int npp = a.pair_npp[pr];
   double I[NA * NB * NA * NB];
-  EriClass<LA, LB, LA, LB>::template eval<BOYS, PURE>(pp, npp, pp, npp, ABx, ABy, ABz, ABx, ABy, ABz, I);
+  EriClass<LA, LB, LA, LB>::template eval<BOYS, PURE>(pp, npp, pp, npp, ABx, ABy, ABz, ABx, ABy, ABz, I,
+                                                      a.boys_cell);
   double mx = 0.0;
 #pragma unroll
   for (int i = 0; i < NA; ++i)

@@ -1,11 +1,22 @@
-"""Generates boys_tab.cuh: F_m(x) on a grid for the fast (exact) Boys mode.
+"""Generates the Boys function tables: boys_tab.cuh (sizes and the small
+tables, defined per translation unit) and boys_cell_data.cu (the one definition
+of the 627 KB cell-record table and the host function that returns its device
+address; kernels receive that address in their argument structs, so the table
+exists once per GPU whatever the number of kernel modules reading it).
 
-Grid x_k = k / 16, k = 0..575 (x < 36), m = 0..23 (24 doubles per point, so the
-seven Taylor coefficients F_{L..L+6}(x_k) a thread needs are contiguous and it
-fetches them with 16-byte loads).  Values come from
-F_m(x) = 1F1(m + 1/2; m + 3/2; -x) / (2m + 1) evaluated with mpmath at 40 digits.
+Tables:
+* g_boys_tab: F_m(x) for the fast (accurate) mode on the grid x_k = k / 16,
+  k = 0..575 (x < 36), m = 0..23 (24 doubles per point, so the seven Taylor
+  coefficients F_{L..L+6}(x_k) a thread needs are contiguous), from
+  F_m(x) = 1F1(m + 1/2; m + 3/2; -x) / (2m + 1) with mpmath at 40 digits.
+* g_boys_bp / g_boys_lp / g_boys_idx: truncation breakpoints of the
+  reference's series (chem/GaussianIntegral.cpp:209-223) and their log
+  products, for the accurate-minus-tail form (boys_ref_walk).
+* g_boys_cell: per-cell Taylor records of the reference's own values
+  (boys_ref_cells), orders 0..8.
+* g_odd_inv: 1/(2k+1).
 
-Usage: python gen_boys_tab.py OUT.cuh
+Usage: python gen_boys_tab.py OUT.cuh OUT_cells.cu
 """
 import sys
 
@@ -16,7 +27,15 @@ NM = 24
 STEP = 16  # points per unit of x
 
 
+def fmt(v) -> str:
+    return repr(v) if isinstance(v, float) else str(v)
+
+
 def main() -> None:
+    out_h, out_cu = sys.argv[1], sys.argv[2]
+    tables = []  # (ctype, name, align, values)
+    defines = []
+
     mpmath.mp.dps = 40
     vals = []
     for k in range(NGRID):
@@ -24,111 +43,120 @@ def main() -> None:
         for m in range(NM):
             v = mpmath.hyp1f1(m + mpmath.mpf(1) / 2, m + mpmath.mpf(3) / 2, -x) / (2 * m + 1)
             vals.append(float(v))
-    with open(sys.argv[1], "w") as f:
-        f.write("// Generated by gen_boys_tab.py -- do not edit.\n#pragma once\n")
-        f.write(f"#define DSS_BOYS_NGRID {NGRID}\n#define DSS_BOYS_NM {NM}\n#define DSS_BOYS_STEP {STEP}\n")
-        f.write("static __device__ const double g_boys_tab[%d] = {\n" % (NGRID * NM))
-        for i in range(0, len(vals), 4):
-            f.write("  " + ", ".join(repr(v) for v in vals[i:i + 4]) + ",\n")
-        f.write("};\n")
-        # Truncation breakpoints of the reference's series (boys.cuh, boys_ref):
-        # for order L the m=L series stops at the first n >= 1 with
-        # t_n = (2x)^n / prod_{j=1..n}(2L+2j+1) <= 1e-9, i.e. at n(x) = 1 + #{k >= 1 : B_L[k] < x}
-        # with B_L[k] = 0.5 exp((ln 1e-9 + LP_L[k]) / k), LP_L[k] = sum_{j=1..k} ln(2L+2j+1).
-        NLB, NB = 16, 160
-        mpmath.mp.dps = 40
-        LP = [[0.0] * (NB + 1) for _ in range(NLB)]
-        BP = [[0.0] * (NB + 1) for _ in range(NLB)]
-        for L in range(NLB):
-            acc = mpmath.mpf(0)
-            prev = mpmath.mpf(-1)
-            for k in range(1, NB + 1):
-                acc += mpmath.log(2 * L + 2 * k + 1)
-                LP[L][k] = float(acc)
-                b = mpmath.mpf("0.5") * mpmath.exp((mpmath.log(mpmath.mpf("1e-9")) + acc) / k)
-                assert b > prev, (L, k)
-                prev = b
-                BP[L][k] = float(b)
-        # Coarse index: for x in [g/4, (g+1)/4): the count of breakpoints below g/4.
-        NG = 200
-        IDX = [[sum(1 for k in range(1, NB + 1) if BP[L][k] < g / 4.0) for g in range(NG)] for L in range(NLB)]
-        f.write(f"#define DSS_BOYS_NLB {NLB}\n#define DSS_BOYS_NB {NB}\n#define DSS_BOYS_NG {NG}\n")
-        for name, tab in (("g_boys_bp", BP), ("g_boys_lp", LP)):
-            f.write("static __device__ const double %s[%d] = {\n" % (name, NLB * (NB + 1)))
-            for L in range(NLB):
-                f.write("  " + ", ".join(repr(v) for v in tab[L]) + ",\n")
-            f.write("};\n")
-        f.write("static __device__ const unsigned char g_boys_idx[%d] = {\n" % (NLB * NG))
-        for L in range(NLB):
-            f.write("  " + ", ".join(str(v) for v in IDX[L]) + ",\n")
-        f.write("};\n")
-        # Reference-mode values without running the series.  Within one interval
-        # I_n = (B_m[n-1], B_m[n]] of order m the reference returns the analytic
-        # function G_{m,n}(x) = exp(-x) sum_{i=0..n} a_i x^i, a_i = 2^i / prod_{j=0..i}(2m+2j+1).
-        # Taylor coefficients G^(j)(x0)/j!, j = 0..6 (8 doubles per node, the 8th 0),
-        # at three kinds of nodes: the grid x0 = k/16 for the interval that holds it
-        # (g_boys_rg, interval index in g_boys_rn), and both ends of every interval
-        # (g_boys_rr: G_{m,n} at B_m[n]; g_boys_rl: G_{m,n} at B_m[n-1]).  A point x of I_n
-        # takes the grid node k = round(16 x) when that node lies in I_n, else the
-        # end of I_n on the node's side, so |x - x0| <= 1/32 always.
-        NLR, NBR = 3, 86
-        mpmath.mp.dps = 30
-        def taylor(m, n, x0):
-            x0 = mpmath.mpf(x0)
-            a = []
-            c = mpmath.mpf(1) / (2 * m + 1)
+    defines += [("DSS_BOYS_NGRID", NGRID), ("DSS_BOYS_NM", NM), ("DSS_BOYS_STEP", STEP)]
+    tables.append(("double", "g_boys_tab", 16, vals))
+
+    # Truncation breakpoints of the reference's series: for order L the m=L
+    # series stops at the first n >= 1 with
+    # t_n = (2x)^n / prod_{j=1..n}(2L+2j+1) <= 1e-9, i.e. at n(x) = 1 + #{k >= 1 : B_L[k] < x}
+    # with B_L[k] = 0.5 exp((ln 1e-9 + LP_L[k]) / k), LP_L[k] = sum_{j=1..k} ln(2L+2j+1).
+    NLB, NB = 16, 160
+    LP = [[0.0] * (NB + 1) for _ in range(NLB)]
+    BP = [[0.0] * (NB + 1) for _ in range(NLB)]
+    for L in range(NLB):
+        acc = mpmath.mpf(0)
+        prev = mpmath.mpf(-1)
+        for k in range(1, NB + 1):
+            acc += mpmath.log(2 * L + 2 * k + 1)
+            LP[L][k] = float(acc)
+            b = mpmath.mpf("0.5") * mpmath.exp((mpmath.log(mpmath.mpf("1e-9")) + acc) / k)
+            assert b > prev, (L, k)
+            prev = b
+            BP[L][k] = float(b)
+    # Coarse index: for x in [g/4, (g+1)/4): the count of breakpoints below g/4.
+    NG = 200
+    IDX = [[sum(1 for k in range(1, NB + 1) if BP[L][k] < g / 4.0) for g in range(NG)] for L in range(NLB)]
+    defines += [("DSS_BOYS_NLB", NLB), ("DSS_BOYS_NB", NB), ("DSS_BOYS_NG", NG)]
+    tables.append(("double", "g_boys_bp", 8, [v for row in BP for v in row]))
+    tables.append(("double", "g_boys_lp", 8, [v for row in LP for v in row]))
+    tables.append(("unsigned char", "g_boys_idx", 1, [v for row in IDX for v in row]))
+
+    # Cell records of the reference's values.  Within one interval
+    # I_n = (B_m[n-1], B_m[n]] of order m the reference returns the analytic
+    # function G_{m,n}(x) = exp(-x) sum_{i=0..n} a_i x^i, a_i = 2^i / prod_{j=0..i}(2m+2j+1);
+    # taylor() gives G_{m,n}^(j)(x0)/j!, j = 0..6.
+    mpmath.mp.dps = 30
+
+    def taylor(m, n, x0):
+        x0 = mpmath.mpf(x0)
+        a = []
+        c = mpmath.mpf(1) / (2 * m + 1)
+        a.append(c)
+        for i in range(1, n + 1):
+            c = c * 2 / (2 * m + 2 * i + 1)
             a.append(c)
-            for i in range(1, n + 1):
-                c = c * 2 / (2 * m + 2 * i + 1)
-                a.append(c)
-            S = []
-            for l in range(7):
-                acc = mpmath.mpf(0)
-                for i in range(l, n + 1):
-                    acc += a[i] * mpmath.binomial(i, l) * x0 ** (i - l)
-                S.append(acc)
-            e = mpmath.exp(-x0)
-            out = []
-            for j in range(7):
-                t = mpmath.mpf(0)
-                for k in range(j + 1):
-                    t += e * (-1) ** k / mpmath.factorial(k) * S[j - k]
-                out.append(float(t))
-            return out + [0.0]
-        def nidx(m, x):
-            return 1 + sum(1 for k in range(1, NB + 1) if BP[m][k] < x)
-        RG, RN, RR, RL = [], [], [], []
-        for m in range(NLR):
-            lim = 1.1 * m + 25 + 1.0
-            for k in range(NGRID):
-                x0 = k / STEP
-                n0 = nidx(m, x0)
-                assert n0 < 256
-                RN.append(n0)
-                RG.extend(taylor(m, n0, x0) if x0 <= lim else [0.0] * 8)
-            assert nidx(m, 1.1 * m + 25 + 1.0 / STEP) < NBR, m
-            for n in range(NBR):
-                if n == 0:
-                    RR.extend([0.0] * 8)
-                    RL.extend([0.0] * 8)
-                    continue
-                RR.extend(taylor(m, n, BP[m][n]))
-                RL.extend(taylor(m, n, BP[m][n - 1] if n >= 2 else 0.0))
-        f.write(f"#define DSS_BOYS_NLR {NLR}\n#define DSS_BOYS_NBR {NBR}\n")
-        for name, tab in (("g_boys_rg", RG), ("g_boys_rr", RR), ("g_boys_rl", RL)):
-            f.write("static __device__ __align__(16) const double %s[%d] = {\n" % (name, len(tab)))
-            for i in range(0, len(tab), 8):
-                f.write("  " + ", ".join(repr(v) for v in tab[i:i + 8]) + ",\n")
+        S = []
+        for l in range(7):
+            acc = mpmath.mpf(0)
+            for i in range(l, n + 1):
+                acc += a[i] * mpmath.binomial(i, l) * x0 ** (i - l)
+            S.append(acc)
+        e = mpmath.exp(-x0)
+        out = []
+        for j in range(7):
+            t = mpmath.mpf(0)
+            for k in range(j + 1):
+                t += e * (-1) ** k / mpmath.factorial(k) * S[j - k]
+            out.append(float(t))
+        return out
+
+    def nidx(m, x):
+        return 1 + sum(1 for k in range(1, NB + 1) if BP[m][k] < x)
+
+    # One 128-byte record per order m and grid point k (cell
+    # [k/16 - 1/32, k/16 + 1/32]).  Away from x = 0 a cell holds at most one
+    # truncation breakpoint b (checked below, with a margin), so the
+    # reference's value in the cell is G_{m,nA} for x <= b and G_{m,nA+1} for
+    # x > b; both are entire functions, so both expand about the cell's own node
+    # x0 = k/16 with |x - x0| <= 1/32.  Record layout (doubles): [0..6] Taylor
+    # coefficients of the x <= b piece, [7] b, [8..14] those of the x > b piece,
+    # [15] b; b = 1e300 when the cell has no breakpoint (both halves then hold
+    # the same piece).  Cell 0 (x < 1/32) holds several breakpoints and is not
+    # tabulated; cells above 16 (1.1 m + 25) + 1 are not used.
+    NMC = 9
+    NCELL = 544
+    MARGIN = 1e-9
+    CELL = []
+    for m in range(NMC):
+        kmax = int(round(STEP * (1.1 * m + 25))) + 1
+        assert kmax < NCELL
+        for k in range(NCELL):
+            if k == 0 or k > kmax:
+                CELL.extend([0.0] * 7 + [1e300] + [0.0] * 7 + [1e300])
+                continue
+            lo, hi = k / STEP - 0.5 / STEP - MARGIN, k / STEP + 0.5 / STEP + MARGIN
+            bs = [BP[m][j] for j in range(1, NB + 1) if lo <= BP[m][j] <= hi]
+            assert len(bs) <= 1, (m, k, bs)
+            x0 = k / STEP
+            if not bs:
+                pa = taylor(m, nidx(m, x0), x0)
+                CELL.extend(pa + [1e300] + pa + [1e300])
+            else:
+                b = bs[0]
+                na = nidx(m, b)  # interval (B[na-1], B[na] = b]
+                CELL.extend(taylor(m, na, x0) + [b] + taylor(m, na + 1, x0) + [b])
+    defines += [("DSS_BOYS_NMC", NMC), ("DSS_BOYS_NCELL", NCELL)]
+    tables.append(("double", "g_odd_inv", 8, [1.0 / (2 * k + 1) for k in range(256)]))
+
+    with open(out_h, "w") as f:
+        f.write("// Generated by gen_boys_tab.py -- do not edit.\n#pragma once\n#include <cuda_runtime.h>\n")
+        for name, v in defines:
+            f.write(f"#define {name} {v}\n")
+        for ctype, name, align, vals in tables:
+            f.write(f"static __device__ __align__({align}) const {ctype} {name}[{len(vals)}] = {{\n")
+            for i in range(0, len(vals), 8):
+                f.write("  " + ", ".join(fmt(v) for v in vals[i:i + 8]) + ",\n")
             f.write("};\n")
-        f.write("static __device__ const unsigned char g_boys_rn[%d] = {\n" % len(RN))
-        for i in range(0, len(RN), 32):
-            f.write("  " + ", ".join(str(v) for v in RN[i:i + 32]) + ",\n")
+        f.write("// Device address of the cell-record table on the current device.\n")
+        f.write("cudaError_t dss_boys_cell_table(const double** out);\n")
+    with open(out_cu, "w") as f:
+        f.write("// Generated by gen_boys_tab.py -- do not edit.\n#include <cuda_runtime.h>\n")
+        f.write(f"static __device__ __align__(128) const double g_boys_cell[{len(CELL)}] = {{\n")
+        for i in range(0, len(CELL), 8):
+            f.write("  " + ", ".join(fmt(v) for v in CELL[i:i + 8]) + ",\n")
         f.write("};\n")
-        f.write("static __device__ const double g_odd_inv[256] = {\n")
-        inv = [1.0 / (2 * k + 1) for k in range(256)]
-        for i in range(0, 256, 4):
-            f.write("  " + ", ".join(repr(v) for v in inv[i:i + 4]) + ",\n")
-        f.write("};\n")
+        f.write("cudaError_t dss_boys_cell_table(const double** out) {\n")
+        f.write("  return cudaGetSymbolAddress((void**)out, g_boys_cell);\n}\n")
 
 
 if __name__ == "__main__":

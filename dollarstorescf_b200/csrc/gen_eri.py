@@ -210,7 +210,7 @@ class ClassGen:
         o(f"template <int BOYS, bool PURE, typename R = double>")
         o(f"__device__ __forceinline__ void eri_{self.name}(const PrimPair* __restrict__ bra, int nbra,")
         o(f"    const PrimPair* __restrict__ ket, int nket, double ABx_, double ABy_, double ABz_,")
-        o(f"    double CDx_, double CDy_, double CDz_, R* __restrict__ I) {{")
+        o(f"    double CDx_, double CDy_, double CDz_, R* __restrict__ I, const double* __restrict__ cells) {{")
         o(f"  const R ABx = (R)ABx_, ABy = (R)ABy_, ABz = (R)ABz_;")
         o(f"  const R CDx = (R)CDx_, CDy = (R)CDy_, CDz = (R)CDz_;")
         o(f"  R acc[{nE * nF}];")
@@ -224,7 +224,7 @@ class ClassGen:
         o(f"      double PAx_, PAy_, PAz_, WPx_, WPy_, WPz_, QCx_, QCy_, QCz_, WQx_, WQy_, WQz_;")
         o(f"      double oo2p_, oo2q_, oo2pq_, rho_p_, rho_q_;")
         o(f"      prim_quartet<BOYS, {L}>(bp, kp, Fd, PAx_, PAy_, PAz_, WPx_, WPy_, WPz_, QCx_, QCy_, QCz_, WQx_,")
-        o(f"                              WQy_, WQz_, oo2p_, oo2q_, oo2pq_, rho_p_, rho_q_);")
+        o(f"                              WQy_, WQz_, oo2p_, oo2q_, oo2pq_, rho_p_, rho_q_, cells);")
         o(f"      R F[{L + 1}];")
         o(f"#pragma unroll")
         o(f"      for (int m = 0; m <= {L}; ++m) F[m] = (R)Fd[m];")

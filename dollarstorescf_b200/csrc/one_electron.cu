@@ -1,9 +1,15 @@
-// One-electron matrices on the host (C++, threads over shell pairs): overlap,
-// kinetic energy and nuclear attraction of the current basis, replacing
-// scf::assignOverlapMatrix / scf::assignCoreHamiltonian
-// (chem/scf/SCFBasis.cpp:56-83) and the integrals they call
-// (overlapIntegral, kineticEnergyIntegral, nuclearPotentialIntegral,
+// One-electron matrices on the device: overlap, kinetic energy and nuclear
+// attraction of a basis, replacing scf::assignOverlapMatrix /
+// scf::assignCoreHamiltonian (chem/scf/SCFBasis.cpp:56-83) and the integrals
+// they call (overlapIntegral, kineticEnergyIntegral, nuclearPotentialIntegral,
 // chem/GaussianIntegral.cpp:29-332).
+//
+// One warp per shell pair, kernels templated on the pair class (l_a >= l_b).
+// The lanes split the primitive pairs (overlap, kinetic) and the (primitive
+// pair, nucleus) combinations (nuclear attraction); the sums are reduced with
+// warp shuffles, after which every lane holds them, runs the horizontal
+// transfer and the Cartesian -> function transform, and writes its share of the
+// packed outputs.
 //
 // Obara-Saika for one centre pair (p = a + b, P the product centre):
 //   overlap, per Cartesian direction:
@@ -14,13 +20,15 @@
 //   nuclear attraction (nucleus C, charge Z, -Z <a| 1/r_C |b>):
 //     [e+1_i]^(m) = PA_i [e]^(m) - PC_i [e]^(m+1) + e_i/(2p) ([e-1_i]^(m) - [e-1_i]^(m+1)),
 //     [0]^(m) = 2 pi / p exp(-ab/p AB^2) F_m(p PC^2), then the horizontal transfer
-//     (a|b+1_i) = (a+1_i|b) + AB_i (a|b); F_m with the reference's series (parity).
+//     (a|b+1_i) = (a+1_i|b) + AB_i (a|b); F_m are the reference's values
+//     (boys_ref, the parity mode of the Boys function).
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <string>
-#include <thread>
 #include <vector>
 
+#include "boys.cuh"
 #include "dss.h"
 #include "dss_internal.h"
 #include "sph_tab.h"
@@ -28,181 +36,412 @@
 namespace {
 
 constexpr double kPiRef = 3.14159265358979;  // lalib/MathUtil.hpp:8
-constexpr int kLmax = 4;                     // per shell on the host path
-constexpr int kNC = (kLmax + 1) * (kLmax + 2) / 2;
+constexpr int kLmaxOne = 2;                  // per shell, as the ERI kernels
 
-int ncart(int l) { return (l + 1) * (l + 2) / 2; }
-int coff(int l) { return l * (l + 1) * (l + 2) / 6; }
-int cidx(int a, int b, int c) {
-  const int l = a + b + c;
-  int pos = 0;
-  for (int ap = l; ap > a; --ap) pos += l - ap + 1;
-  return pos + (l - a - b);
-}
-int call_idx(int a, int b, int c) { return coff(a + b + c) + cidx(a, b, c); }
-
-struct Cart3 {
-  int x, y, z;
-};
-std::vector<std::vector<Cart3>> cart_tables() {
-  std::vector<std::vector<Cart3>> t(2 * kLmax + 2);
-  for (int l = 0; l < (int)t.size(); ++l)
-    for (int a = l; a >= 0; --a)
-      for (int b = l - a; b >= 0; --b) t[l].push_back({a, b, l - a - b});
-  return t;
-}
-
-// The reference's Boys function (chem/GaussianIntegral.cpp:209-223).
-double boys_ref_host(double x, unsigned m) {
-  if (x > (double)m * 1.1 + 25.0) {
-    unsigned int dfi = 1u;
-    for (int j = 2 * (int)m - 1; j > 0; j -= 2) dfi *= (unsigned int)j;
-    double p2 = 1.0;
-    for (unsigned j = 0; j < m + 1; ++j) p2 *= 2.0;
-    // integer power in the reference's square-and-multiply order
-    unsigned p = 2 * m + 1;
-    double fac[8];
-    int nf = 0;
-    double tail;
-    while (true) {
-      if (p == 0) { tail = 1.0; break; }
-      if (p == 1) { tail = x; break; }
-      double y = x;
-      unsigned l = 2;
-      for (; l < p; l *= 2) y = y * y;
-      fac[nf++] = y;
-      p -= l / 2;
+__host__ __device__ constexpr int oe_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int oe_coff(int l) { return l * (l + 1) * (l + 2) / 6; }
+// Exponents of the k-th Cartesian monomial of degree l (x-major: x power
+// descending, then y power descending).
+__host__ __device__ constexpr int oe_cx(int l, int k) {
+  int idx = 0;
+  for (int a = l; a >= 0; --a)
+    for (int b = l - a; b >= 0; --b) {
+      if (idx == k) return a;
+      ++idx;
     }
-    double r = tail;
-    for (int i = nf - 1; i >= 0; --i) r = fac[i] * r;
-    return (double)(int)dfi / p2 * std::sqrt(kPiRef / r);
-  }
-  double F = 1.0, a = 1.0;
-  for (int i = 1; a > 0.000000001; ++i) {
-    a = 2.0 * x / (double)(2 * (int)m + 2 * i + 1) * a;
-    F += a;
-  }
-  return std::exp(-x) / (double)(2 * m + 1) * F;
+  return 0;
+}
+__host__ __device__ constexpr int oe_cy(int l, int k) {
+  int idx = 0;
+  for (int a = l; a >= 0; --a)
+    for (int b = l - a; b >= 0; --b) {
+      if (idx == k) return b;
+      ++idx;
+    }
+  return 0;
+}
+// Index of x^a y^b z^c among all monomials of degree <= a + b + c.
+__host__ __device__ constexpr int oe_idx(int a, int b, int c) {
+  int pos = oe_coff(a + b + c);
+  for (int ap = a + b + c; ap > a; --ap) pos += a + b + c - ap + 1;
+  return pos + c;
 }
 
-struct PairOut {
-  // Cartesian blocks [ncart(la)][ncart(lb)]
-  double S[kNC * kNC], T[kNC * kNC], V[kNC * kNC];
+struct OneEArgs {
+  const int2* pairs;  // (shell with the larger l, other shell)
+  int npair;
+  const int* sh_l;
+  const int* sh_nprim;
+  const int* sh_prim0;
+  const int* sh_f0;
+  const double* sh_xyz;
+  const double* exps;
+  const double* wts;
+  int natom;
+  const double* atom_xyz;
+  const double* atom_z;
+  const double* tr;  // [l][function][Cartesian], 6 x 6 per l
+  int pure;
+  double* S;  // packed-U outputs; V == NULL: T receives T + V (the core Hamiltonian)
+  double* T;
+  double* V;
+  const double* boys_cell;  // reference-mode Boys records (dss_boys_cell_table)
 };
 
-void pair_integrals(const BasisHost& B, int sa, int sb, int natom, const int* Z, const double* xyz,
-                    const std::vector<std::vector<Cart3>>& ct, PairOut& out) {
-  const int la = B.l[sa], lb = B.l[sb];
-  const int na = ncart(la), nb = ncart(lb);
-  std::memset(&out, 0, sizeof(out));
-  const double* A = &B.xyz[3 * sa];
-  const double* Bc = &B.xyz[3 * sb];
-  const double AB[3] = {A[0] - Bc[0], A[1] - Bc[1], A[2] - Bc[2]};
+__device__ __forceinline__ double oe_warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(128) one_e_kernel(OneEArgs a) {
+  constexpr int NA = oe_ncart(LA), NB = oe_ncart(LB);
+  constexpr int E = LA + LB;
+  constexpr int NE = oe_coff(E + 1);
+  constexpr int NBC = oe_coff(LB + 1);
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (warp >= a.npair) return;  // uniform per warp
+  const int2 pr = a.pairs[warp];
+  const int sa = pr.x, sb = pr.y;
+  const double A[3] = {a.sh_xyz[3 * sa], a.sh_xyz[3 * sa + 1], a.sh_xyz[3 * sa + 2]};
+  const double B[3] = {a.sh_xyz[3 * sb], a.sh_xyz[3 * sb + 1], a.sh_xyz[3 * sb + 2]};
+  const double AB[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
   const double AB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
-  const int E = la + lb;
-  const int nE = coff(E + 1);
-  const int nBc = coff(lb + 1);
-  std::vector<double> Vt((size_t)(E + 1) * nE), acc(nE, 0.0), br((size_t)nE * nBc);
-  for (int i = 0; i < B.nprim[sa]; ++i)
-    for (int j = 0; j < B.nprim[sb]; ++j) {
-      const double al = B.exps[B.prim0[sa] + i], be = B.exps[B.prim0[sb] + j];
-      const double w = B.wts[B.prim0[sa] + i] * B.wts[B.prim0[sb] + j];
-      const double p = al + be, mu = al * be / p;
-      double P[3], PA[3], PB[3];
-      for (int k = 0; k < 3; ++k) {
-        P[k] = (al * A[k] + be * Bc[k]) / p;
-        PA[k] = P[k] - A[k];
-        PB[k] = P[k] - Bc[k];
-      }
-      // 1-D overlaps up to (la, lb + 2)
-      double Sd[3][kLmax + 2][kLmax + 4];
-      for (int d = 0; d < 3; ++d) {
-        Sd[d][0][0] = std::sqrt(kPiRef / p) * std::exp(-mu * AB[d] * AB[d]);
-        for (int ii = 0; ii <= la + 1; ++ii)
-          for (int jj = 0; jj <= lb + 2; ++jj) {
-            if (ii == 0 && jj == 0) continue;
-            double v;
-            if (ii > 0) {
-              v = PA[d] * Sd[d][ii - 1][jj];
-              if (ii > 1) v += (ii - 1) * Sd[d][ii - 2][jj] / (2.0 * p);
-              if (jj > 0) v += jj * Sd[d][ii - 1][jj - 1] / (2.0 * p);
-            } else {
-              v = PB[d] * Sd[d][0][jj - 1];
-              if (jj > 1) v += (jj - 1) * Sd[d][0][jj - 2] / (2.0 * p);
-            }
-            Sd[d][ii][jj] = v;
-          }
-      }
-      for (int ia = 0; ia < na; ++ia)
-        for (int ib = 0; ib < nb; ++ib) {
-          const int ea[3] = {ct[la][ia].x, ct[la][ia].y, ct[la][ia].z};
-          const int eb[3] = {ct[lb][ib].x, ct[lb][ib].y, ct[lb][ib].z};
-          const double sx = Sd[0][ea[0]][eb[0]], sy = Sd[1][ea[1]][eb[1]], sz = Sd[2][ea[2]][eb[2]];
-          out.S[ia * nb + ib] += w * sx * sy * sz;
-          double t = 0.0;
-          for (int d = 0; d < 3; ++d) {
-            const int jj = eb[d], ii = ea[d];
-            double k = -2.0 * be * (2 * jj + 1) * Sd[d][ii][jj] + 4.0 * be * be * Sd[d][ii][jj + 2];
-            if (jj > 1) k += jj * (jj - 1) * Sd[d][ii][jj - 2];
-            double o = 1.0;
-            for (int d2 = 0; d2 < 3; ++d2)
-              if (d2 != d) o *= Sd[d2][ea[d2]][eb[d2]];
-            t += -0.5 * k * o;
-          }
-          out.T[ia * nb + ib] += w * t;
-        }
-      // nuclear attraction
-      const double pref = 2.0 * kPiRef / p * std::exp(-mu * AB2) * w;
-      for (int c = 0; c < natom; ++c) {
-        const double* C = &xyz[3 * c];
-        double PC[3] = {P[0] - C[0], P[1] - C[1], P[2] - C[2]};
-        const double x = p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
-        for (int m = 0; m <= E; ++m) Vt[(size_t)m * nE] = pref * boys_ref_host(x, (unsigned)m);
-        for (int e = 1; e <= E; ++e)
-          for (const Cart3& q : ct[e]) {
-            int em[3] = {q.x, q.y, q.z};
-            const int dir = q.x ? 0 : (q.y ? 1 : 2);
-            em[dir] -= 1;
-            const int i1 = call_idx(em[0], em[1], em[2]);
-            int i2 = -1;
-            if (em[dir] > 0) {
-              int e2[3] = {em[0], em[1], em[2]};
-              e2[dir] -= 1;
-              i2 = call_idx(e2[0], e2[1], e2[2]);
-            }
-            const int it = call_idx(q.x, q.y, q.z);
-            for (int m = 0; m <= E - e; ++m) {
-              double v = PA[dir] * Vt[(size_t)m * nE + i1] - PC[dir] * Vt[(size_t)(m + 1) * nE + i1];
-              if (i2 >= 0) v += em[dir] / (2.0 * p) * (Vt[(size_t)m * nE + i2] - Vt[(size_t)(m + 1) * nE + i2]);
-              Vt[(size_t)m * nE + it] = v;
-            }
-          }
-        for (int e = 0; e < nE; ++e) acc[e] += -(double)Z[c] * Vt[e];
-      }
+  const int npa = a.sh_nprim[sa], npb = a.sh_nprim[sb];
+  const int pa0 = a.sh_prim0[sa], pb0 = a.sh_prim0[sb];
+  const int npp = npa * npb;
+
+  double S[NA * NB], T[NA * NB], Vacc[NE];
+#pragma unroll
+  for (int q = 0; q < NA * NB; ++q) S[q] = T[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < NE; ++q) Vacc[q] = 0.0;
+
+  // Overlap and kinetic energy: lanes over primitive pairs.
+  for (int t = lane; t < npp; t += 32) {
+    const int i = t / npb, j = t - (t / npb) * npb;
+    const double al = a.exps[pa0 + i], be = a.exps[pb0 + j];
+    const double w = a.wts[pa0 + i] * a.wts[pb0 + j];
+    const double p = al + be, mu = al * be / p;
+    double PA[3], PB[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double P = (al * A[d] + be * B[d]) / p;
+      PA[d] = P - A[d];
+      PB[d] = P - B[d];
     }
-  // horizontal transfer of the accumulated nuclear integrals
-  for (int e = 0; e < nE; ++e) br[(size_t)e * nBc] = acc[e];
-  for (int bd = 1; bd <= lb; ++bd)
-    for (const Cart3& q : ct[bd]) {
-      int bm[3] = {q.x, q.y, q.z};
-      const int dir = q.x ? 0 : (q.y ? 1 : 2);
-      bm[dir] -= 1;
-      const int ibm = call_idx(bm[0], bm[1], bm[2]), ibt = call_idx(q.x, q.y, q.z);
+    double Sd[3][LA + 1][LB + 3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      Sd[d][0][0] = sqrt(kPiRef / p) * exp(-mu * AB[d] * AB[d]);
+#pragma unroll
+      for (int ii = 0; ii <= LA; ++ii)
+#pragma unroll
+        for (int jj = 0; jj <= LB + 2; ++jj) {
+          if (ii == 0 && jj == 0) continue;
+          double v;
+          if (ii > 0) {
+            v = PA[d] * Sd[d][ii - 1][jj];
+            if (ii > 1) v += (ii - 1) * Sd[d][ii - 2][jj] / (2.0 * p);
+            if (jj > 0) v += jj * Sd[d][ii - 1][jj - 1] / (2.0 * p);
+          } else {
+            v = PB[d] * Sd[d][0][jj - 1];
+            if (jj > 1) v += (jj - 1) * Sd[d][0][jj - 2] / (2.0 * p);
+          }
+          Sd[d][ii][jj] = v;
+        }
+    }
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) {
+        const int ea[3] = {oe_cx(LA, ia), oe_cy(LA, ia), LA - oe_cx(LA, ia) - oe_cy(LA, ia)};
+        const int eb[3] = {oe_cx(LB, ib), oe_cy(LB, ib), LB - oe_cx(LB, ib) - oe_cy(LB, ib)};
+        const double sx = Sd[0][ea[0]][eb[0]], sy = Sd[1][ea[1]][eb[1]], sz = Sd[2][ea[2]][eb[2]];
+        S[ia * NB + ib] += w * sx * sy * sz;
+        double tk = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const int jj = eb[d], ii = ea[d];
+          double k = -2.0 * be * (2 * jj + 1) * Sd[d][ii][jj] + 4.0 * be * be * Sd[d][ii][jj + 2];
+          if (jj > 1) k += jj * (jj - 1) * Sd[d][ii][jj - 2];
+          double o = 1.0;
+#pragma unroll
+          for (int d2 = 0; d2 < 3; ++d2)
+            if (d2 != d) o *= Sd[d2][ea[d2]][eb[d2]];
+          tk += -0.5 * k * o;
+        }
+        T[ia * NB + ib] += w * tk;
+      }
+  }
+
+  // Nuclear attraction: lanes over (primitive pair, nucleus).
+  const int nwork = npp * a.natom;
+  for (int t = lane; t < nwork; t += 32) {
+    const int q = t / a.natom, c = t - (t / a.natom) * a.natom;
+    const int i = q / npb, j = q - (q / npb) * npb;
+    const double al = a.exps[pa0 + i], be = a.exps[pb0 + j];
+    const double w = a.wts[pa0 + i] * a.wts[pb0 + j];
+    const double p = al + be, mu = al * be / p;
+    double PA[3], PC[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double P = (al * A[d] + be * B[d]) / p;
+      PA[d] = P - A[d];
+      PC[d] = P - a.atom_xyz[3 * c + d];
+    }
+    const double pref = 2.0 * kPiRef / p * exp(-mu * AB2) * w;
+    const double x = p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
+    double F[E + 1];
+    boys_ref<E>(x, F, a.boys_cell);
+    double Vt[E + 1][NE];
+#pragma unroll
+    for (int m = 0; m <= E; ++m) Vt[m][0] = pref * F[m];
+#pragma unroll
+    for (int e = 1; e <= E; ++e)
+#pragma unroll
+      for (int k = 0; k < oe_ncart(e); ++k) {
+        const int qx = oe_cx(e, k), qy = oe_cy(e, k), qz = e - qx - qy;
+        const int dir = qx ? 0 : (qy ? 1 : 2);
+        const int mx = qx - (dir == 0), my = qy - (dir == 1), mz = qz - (dir == 2);
+        const int edir = dir == 0 ? mx : (dir == 1 ? my : mz);
+        const int i1 = oe_idx(mx, my, mz);
+        const int it = oe_idx(qx, qy, qz);
+#pragma unroll
+        for (int m = 0; m <= E - e; ++m) {
+          double v = PA[dir] * Vt[m][i1] - PC[dir] * Vt[m + 1][i1];
+          if (edir > 0) {
+            const int i2 = oe_idx(mx - (dir == 0), my - (dir == 1), mz - (dir == 2));
+            v += edir / (2.0 * p) * (Vt[m][i2] - Vt[m + 1][i2]);
+          }
+          Vt[m][it] = v;
+        }
+      }
+    const double z = a.atom_z[c];
+#pragma unroll
+    for (int e = 0; e < NE; ++e) Vacc[e] += -z * Vt[0][e];
+  }
+
+#pragma unroll
+  for (int q = 0; q < NA * NB; ++q) {
+    S[q] = oe_warp_sum(S[q]);
+    T[q] = oe_warp_sum(T[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < NE; ++q) Vacc[q] = oe_warp_sum(Vacc[q]);
+
+  // Horizontal transfer of the nuclear integrals to (a|b).
+  double br[NE][NBC];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) br[e][0] = Vacc[e];
+#pragma unroll
+  for (int bd = 1; bd <= LB; ++bd)
+#pragma unroll
+    for (int k = 0; k < oe_ncart(bd); ++k) {
+      const int qx = oe_cx(bd, k), qy = oe_cy(bd, k), qz = bd - qx - qy;
+      const int dir = qx ? 0 : (qy ? 1 : 2);
+      const int ibm = oe_idx(qx - (dir == 0), qy - (dir == 1), qz - (dir == 2));
+      const int ibt = oe_idx(qx, qy, qz);
+#pragma unroll
       for (int ed = 0; ed <= E - bd; ++ed)
-        for (const Cart3& r : ct[ed]) {
-          int ec[3] = {r.x, r.y, r.z};
-          const int ie = call_idx(r.x, r.y, r.z);
-          ec[dir] += 1;
-          const int iep = call_idx(ec[0], ec[1], ec[2]);
-          br[(size_t)ie * nBc + ibt] = br[(size_t)iep * nBc + ibm] + AB[dir] * br[(size_t)ie * nBc + ibm];
+#pragma unroll
+        for (int r = 0; r < oe_ncart(ed); ++r) {
+          const int rx = oe_cx(ed, r), ry = oe_cy(ed, r), rz = ed - rx - ry;
+          const int ie = oe_idx(rx, ry, rz);
+          const int iep = oe_idx(rx + (dir == 0), ry + (dir == 1), rz + (dir == 2));
+          br[ie][ibt] = br[iep][ibm] + AB[dir] * br[ie][ibm];
         }
     }
-  for (int ia = 0; ia < na; ++ia)
-    for (int ib = 0; ib < nb; ++ib)
-      out.V[ia * nb + ib] = br[(size_t)(coff(la) + ia) * nBc + coff(lb) + ib];
+
+  // Functions: pure (m = -l..l) or Cartesian, through the transform table.
+  const int nfa = a.pure ? 2 * LA + 1 : NA, nfb = a.pure ? 2 * LB + 1 : NB;
+  const int fa0 = a.sh_f0[sa], fb0 = a.sh_f0[sb];
+  const double* ta = a.tr + LA * 36;
+  const double* tb = a.tr + LB * 36;
+  for (int o = lane; o < nfa * nfb; o += 32) {
+    const int fa = o / nfb, fb = o - (o / nfb) * nfb;
+    const int i = fa0 + fa, j = fb0 + fb;
+    if (sa == sb && j > i) continue;
+    double s = 0.0, tt = 0.0, v = 0.0;
+#pragma unroll
+    for (int ca = 0; ca < NA; ++ca) {
+      const double wa = ta[fa * 6 + ca];
+      if (wa == 0.0) continue;
+#pragma unroll
+      for (int cb = 0; cb < NB; ++cb) {
+        const double wgt = wa * tb[fb * 6 + cb];
+        if (wgt == 0.0) continue;
+        s += wgt * S[ca * NB + cb];
+        tt += wgt * T[ca * NB + cb];
+        v += wgt * br[oe_coff(LA) + ca][oe_coff(LB) + cb];
+      }
+    }
+    const int x = i > j ? i : j, y = i > j ? j : i;
+    const size_t idx = (size_t)x * (x + 1) / 2 + y;
+    if (a.S) a.S[idx] = s;
+    if (a.V) {
+      a.T[idx] = tt;
+      a.V[idx] = v;
+    } else {
+      a.T[idx] = tt + v;
+    }
+  }
+}
+
+template <int LA, int LB>
+void launch_one_e(const OneEArgs& a, cudaStream_t s) {
+  const unsigned blocks = (unsigned)(((long long)a.npair * 32 + 127) / 128);
+  if (blocks) one_e_kernel<LA, LB><<<blocks, 128, 0, s>>>(a);
+}
+
+void launch_one_e_class(int la, int lb, const OneEArgs& a, cudaStream_t s) {
+  switch (la * 3 + lb) {
+    case 0: return launch_one_e<0, 0>(a, s);
+    case 3: return launch_one_e<1, 0>(a, s);
+    case 4: return launch_one_e<1, 1>(a, s);
+    case 6: return launch_one_e<2, 0>(a, s);
+    case 7: return launch_one_e<2, 1>(a, s);
+    case 8: return launch_one_e<2, 2>(a, s);
+    default: return;
+  }
 }
 
 }  // namespace
+
+int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz_bohr,
+                            double* dS, double* dT, double* dV, std::string* errp) {
+  const int ns = (int)B.l.size();
+  for (int q = 0; q < ns; ++q)
+    if (B.l[q] < 0 || B.l[q] > kLmaxOne) {
+      if (errp) *errp = "dss_one_electron: l above 2";
+      return DSS_ERR_UNSUPPORTED;
+    }
+  // Transform tables [l][function][Cartesian] for the basis' 5D/6D choice.
+  std::vector<double> tr((kLmaxOne + 1) * 36, 0.0);
+  for (int t = 0; t < kDssSphTermCount; ++t) {
+    const DssSphTerm& q = kDssSphTerms[t];
+    if (q.pure == B.pure && q.l <= kLmaxOne) tr[q.l * 36 + q.func * 6 + q.cart] = q.w;
+  }
+  // Shell pairs grouped by class, the larger l first.
+  std::vector<std::vector<int2>> cls(9);
+  for (int x = 0; x < ns; ++x)
+    for (int y = 0; y <= x; ++y) {
+      const int a = B.l[y] > B.l[x] ? y : x, b = a == x ? y : x;
+      cls[B.l[a] * 3 + B.l[b]].push_back(make_int2(a, b));
+    }
+  std::vector<int2> pairs;
+  std::vector<size_t> c0(10, 0);
+  for (int c = 0; c < 9; ++c) {
+    c0[c] = pairs.size();
+    pairs.insert(pairs.end(), cls[c].begin(), cls[c].end());
+  }
+  c0[9] = pairs.size();
+  std::vector<double> zd(natom);
+  for (int c = 0; c < natom; ++c) zd[c] = (double)Z[c];
+  // One upload of every input.
+  const size_t ni = 4 * (size_t)ns, nd = 3 * (size_t)ns + 2 * B.exps.size() + 4 * (size_t)natom + tr.size();
+  std::vector<int> hi(ni);
+  std::vector<double> hd;
+  hd.reserve(nd);
+  for (int q = 0; q < ns; ++q) {
+    hi[q] = B.l[q];
+    hi[ns + q] = B.nprim[q];
+    hi[2 * ns + q] = B.prim0[q];
+    hi[3 * ns + q] = B.f0[q];
+  }
+  hd.insert(hd.end(), B.xyz.begin(), B.xyz.end());
+  hd.insert(hd.end(), B.exps.begin(), B.exps.end());
+  hd.insert(hd.end(), B.wts.begin(), B.wts.end());
+  hd.insert(hd.end(), xyz_bohr, xyz_bohr + 3 * (size_t)natom);
+  hd.insert(hd.end(), zd.begin(), zd.end());
+  hd.insert(hd.end(), tr.begin(), tr.end());
+  DevBuf<int2> d_pairs;
+  DevBuf<int> d_i;
+  DevBuf<double> d_d;
+  cudaError_t e = d_pairs.resize(std::max<size_t>(pairs.size(), 1));
+  if (e == cudaSuccess) e = d_i.resize(std::max<size_t>(ni, 1));
+  if (e == cudaSuccess) e = d_d.resize(std::max<size_t>(hd.size(), 1));
+  if (e == cudaSuccess && !pairs.empty())
+    e = cudaMemcpyAsync(d_pairs.ptr, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && ni) e = cudaMemcpyAsync(d_i.ptr, hi.data(), ni * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !hd.empty())
+    e = cudaMemcpyAsync(d_d.ptr, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) {
+    if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? DSS_ERR_OOM : DSS_ERR_CUDA;
+  }
+  OneEArgs a;
+  a.sh_l = d_i.ptr;
+  a.sh_nprim = d_i.ptr + ns;
+  a.sh_prim0 = d_i.ptr + 2 * ns;
+  a.sh_f0 = d_i.ptr + 3 * ns;
+  a.sh_xyz = d_d.ptr;
+  a.exps = a.sh_xyz + 3 * ns;
+  a.wts = a.exps + B.exps.size();
+  a.atom_xyz = a.wts + B.exps.size();
+  a.atom_z = a.atom_xyz + 3 * (size_t)natom;
+  a.tr = a.atom_z + natom;
+  a.natom = natom;
+  a.pure = B.pure;
+  a.S = dS;
+  a.T = dT;
+  a.V = dV;
+  e = dss_boys_cell_table(&a.boys_cell);
+  if (e != cudaSuccess) {
+    if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
+    return DSS_ERR_CUDA;
+  }
+  for (int c = 0; c < 9; ++c) {
+    if (c0[c + 1] == c0[c]) continue;
+    a.pairs = d_pairs.ptr + c0[c];
+    a.npair = (int)(c0[c + 1] - c0[c]);
+    launch_one_e_class(c / 3, c % 3, a, s);
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the input buffers are freed on return
+  if (e != cudaSuccess) {
+    if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
+    return DSS_ERR_CUDA;
+  }
+  return DSS_OK;
+}
+
+double dss_nuclear_repulsion(int natom, const int* Z, const double* xyz_bohr) {
+  // sum_{A<B} Z_A Z_B / R_AB (chem/scf/Energy.cpp:44-49)
+  double e = 0.0;
+  for (int i = 0; i < natom; ++i)
+    for (int j = i + 1; j < natom; ++j) {
+      const double dx = xyz_bohr[3 * i] - xyz_bohr[3 * j], dy = xyz_bohr[3 * i + 1] - xyz_bohr[3 * j + 1],
+                   dz = xyz_bohr[3 * i + 2] - xyz_bohr[3 * j + 2];
+      e += (double)Z[i] * Z[j] / std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  return e;
+}
+
+int dss_one_electron_basis(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz_bohr,
+                           double* S_packed, double* T_packed, double* V_packed, double* e_nuc, std::string* errp) {
+  const size_t np = (size_t)B.nbf * (B.nbf + 1) / 2;
+  DevBuf<double> d;
+  cudaError_t e = d.resize(std::max<size_t>(3 * np, 1));
+  if (e != cudaSuccess) {
+    if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
+    return DSS_ERR_OOM;
+  }
+  int rc = dss_one_electron_device(s, B, natom, Z, xyz_bohr, d.ptr, d.ptr + np, d.ptr + 2 * np, errp);
+  if (rc != DSS_OK) return rc;
+  double* outs[3] = {S_packed, T_packed, V_packed};
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+    if (outs[k] && np) e = cudaMemcpyAsync(outs[k], d.ptr + k * np, np * 8, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
+    return DSS_ERR_CUDA;
+  }
+  if (e_nuc) *e_nuc = dss_nuclear_repulsion(natom, Z, xyz_bohr);
+  return DSS_OK;
+}
 
 extern "C" int dss_one_electron(dss_ctx* ctx, int natom, const int* Z, const double* xyz_bohr, double* S_packed,
                                 double* T_packed, double* V_packed, double* e_nuc) {
@@ -211,86 +450,10 @@ extern "C" int dss_one_electron(dss_ctx* ctx, int natom, const int* Z, const dou
   if (!ctx->nbf || ctx->nmol > 0) return dss_fail(ctx, DSS_ERR_INVALID, "dss_one_electron: no single-molecule basis set");
   if (natom < 0 || (natom > 0 && (!Z || !xyz_bohr)))
     return dss_fail(ctx, DSS_ERR_INVALID, "dss_one_electron: bad atom arrays");
+  cudaSetDevice(ctx->opts.device);
   std::string err;
-  const int rc = dss_one_electron_basis(ctx->basis, natom, Z, xyz_bohr, S_packed, T_packed, V_packed, e_nuc, &err);
+  const int rc = dss_one_electron_basis(ctx->stream, ctx->basis, natom, Z, xyz_bohr, S_packed, T_packed, V_packed,
+                                        e_nuc, &err);
   if (rc != DSS_OK) return dss_fail(ctx, rc, err);
-  return DSS_OK;
-}
-
-int dss_one_electron_basis(const BasisHost& B, int natom, const int* Z, const double* xyz_bohr, double* S_packed,
-                           double* T_packed, double* V_packed, double* e_nuc, std::string* errp) {
-  const int ns = (int)B.l.size();
-  for (int s = 0; s < ns; ++s)
-    if (B.l[s] > kLmax) {
-      if (errp) *errp = "dss_one_electron: l above 4";
-      return DSS_ERR_UNSUPPORTED;
-    }
-  // Function transforms per (l, pure).
-  std::vector<std::vector<std::vector<std::pair<int, double>>>> tr(kLmax + 1);
-  for (int l = 0; l <= kLmax; ++l) tr[l].resize(B.pure ? 2 * l + 1 : ncart(l));
-  for (int t = 0; t < kDssSphTermCount; ++t) {
-    const DssSphTerm& q = kDssSphTerms[t];
-    if (q.pure == B.pure && q.l <= kLmax) tr[q.l][q.func].push_back({q.cart, q.w});
-  }
-  const auto ct = cart_tables();
-  const int n = B.nbf;
-  const size_t np = (size_t)n * (n + 1) / 2;
-  std::vector<double> S(np, 0.0), T(np, 0.0), V(np, 0.0);
-  // Shell pairs (a >= b) split over host threads.
-  std::vector<std::pair<int, int>> pairs;
-  for (int a = 0; a < ns; ++a)
-    for (int b = 0; b <= a; ++b) pairs.push_back({a, b});
-  unsigned nth = std::thread::hardware_concurrency();
-  if (nth == 0) nth = 1;
-  if (nth > 32) nth = 32;
-  auto work = [&](unsigned tid) {
-    PairOut po;
-    for (size_t k = tid; k < pairs.size(); k += nth) {
-      const int sa = pairs[k].first, sb = pairs[k].second;
-      pair_integrals(B, sa, sb, natom, Z, xyz_bohr, ct, po);
-      const int la = B.l[sa], lb = B.l[sb];
-      const int nca = ncart(la), ncb = ncart(lb);
-      const auto& ta = tr[la];
-      const auto& tb = tr[lb];
-      for (size_t fa = 0; fa < ta.size(); ++fa)
-        for (size_t fb = 0; fb < tb.size(); ++fb) {
-          const int i = B.f0[sa] + (int)fa, j = B.f0[sb] + (int)fb;
-          if (sa == sb && j > i) continue;
-          double s = 0.0, t = 0.0, v = 0.0;
-          for (const auto& xa : ta[fa])
-            for (const auto& xb : tb[fb]) {
-              const double wgt = xa.second * xb.second;
-              const int q = xa.first * ncb + xb.first;
-              s += wgt * po.S[q];
-              t += wgt * po.T[q];
-              v += wgt * po.V[q];
-            }
-          (void)nca;
-          const int x = i > j ? i : j, y = i > j ? j : i;
-          const size_t idx = (size_t)x * (x + 1) / 2 + y;
-          S[idx] = s;
-          T[idx] = t;
-          V[idx] = v;
-        }
-    }
-  };
-  std::vector<std::thread> th;
-  for (unsigned t = 1; t < nth; ++t) th.emplace_back(work, t);
-  work(0);
-  for (auto& t : th) t.join();
-  if (S_packed) std::memcpy(S_packed, S.data(), np * 8);
-  if (T_packed) std::memcpy(T_packed, T.data(), np * 8);
-  if (V_packed) std::memcpy(V_packed, V.data(), np * 8);
-  if (e_nuc) {
-    // sum_{A<B} Z_A Z_B / R_AB (chem/scf/Energy.cpp:44-49)
-    double e = 0.0;
-    for (int i = 0; i < natom; ++i)
-      for (int j = i + 1; j < natom; ++j) {
-        const double dx = xyz_bohr[3 * i] - xyz_bohr[3 * j], dy = xyz_bohr[3 * i + 1] - xyz_bohr[3 * j + 1],
-                     dz = xyz_bohr[3 * i + 2] - xyz_bohr[3 * j + 2];
-        e += (double)Z[i] * Z[j] / std::sqrt(dx * dx + dy * dy + dz * dz);
-      }
-    *e_nuc = e;
-  }
   return DSS_OK;
 }

@@ -222,6 +222,34 @@ __global__ void energy_kernel(const double* eps, int nocc, const double* trDG, d
 
 inline unsigned nb(long long N, int t = 256) { return (unsigned)((N + t - 1) / t); }
 
+// UHF two-electron parts from the J/K accumulators of the two spin densities:
+// G_a = J[D_a + D_b] - K[D_a], G_b = J[D_a + D_b] - K[D_b], with
+// J = Ja + Ja^T + Jb + Jb^T and K_s = Ks + Ks^T.  Also J itself (for the energy).
+__global__ void uhf_combine(const double* __restrict__ Ja, const double* __restrict__ Ka,
+                            const double* __restrict__ Jb, const double* __restrict__ Kb, double* __restrict__ Ga,
+                            double* __restrict__ Gb, double* __restrict__ Jt, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  const long long u = (long long)c * n + r;
+  const double J = Ja[t] + Ja[u] + Jb[t] + Jb[u];
+  Ga[t] = J - (Ka[t] + Ka[u]);
+  Gb[t] = J - (Kb[t] + Kb[u]);
+  if (Jt) Jt[t] = J;
+}
+
+// E_elec = sum_{i<na} eps_a_i + sum_{i<nb} eps_b_i - (tr(Da Ga) + tr(Db Gb)) / 2
+// (getTotalElectronicEnergy, unrestricted branch, SCFSolver.cpp:131-142).
+__global__ void uhf_energy_kernel(const double* eps_a, int na, const double* eps_b, int nbeta, const double* tr,
+                                  double* out) {
+  double s = 0.0;
+  for (int i = 0; i < na; ++i) s += eps_a[i];
+  for (int i = 0; i < nbeta; ++i) s += eps_b[i];
+  out[0] = s - 0.5 * tr[0] - 0.5 * tr[1];
+}
+
+
+
 }  // namespace
 
 extern "C" {
@@ -420,6 +448,182 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
   *E_total = 2.0 * tr[0] + tr[1] + e_nuc;
   if (iterations) *iterations = it;
 #undef SCF_CHECK
+  return rc;
+}
+
+
+int dss_uhf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha, int n_beta, double e_nuc,
+                  const dss_scf_opts* opts_in, double* E_total, double* Dap, double* Dbp, int* iterations) {
+  if (!ctx) return DSS_ERR_INVALID;
+  ctx->err.clear();
+  if (!ctx->nbf || ctx->nmol > 0) return dss_fail(ctx, DSS_ERR_INVALID, "dss_uhf_solve: no single-molecule basis set");
+  if (!Hp || !Sp || !E_total) return dss_fail(ctx, DSS_ERR_INVALID, "dss_uhf_solve: NULL argument");
+  const int n = ctx->nbf;
+  if (n_alpha < 0 || n_alpha > n || n_beta < 0 || n_beta > n)
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_uhf_solve: occupied count out of range");
+  dss_scf_opts o;
+  dss_default_scf_opts(&o);
+  if (opts_in) o = *opts_in;
+  if (o.diis_size < 1 || o.diis_size > 9)
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_uhf_solve: diis_size must be 1..9");
+  if (o.incremental) return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_uhf_solve: the incremental form is RHF only");
+  if (o.use_guess && (!Dap || !Dbp)) return dss_fail(ctx, DSS_ERR_INVALID, "dss_uhf_solve: use_guess needs both D");
+  if (cudaSetDevice(ctx->opts.device) != cudaSuccess) return dss_fail(ctx, DSS_ERR_CUDA, "dss_uhf_solve: cudaSetDevice");
+  const size_t n2 = (size_t)n * n, np = (size_t)n * (n + 1) / 2;
+  cudaStream_t s = ctx->stream;
+  ScfBuffers& b = ctx->scf;
+  const int ds = o.diis_size;
+  const size_t need = n2 * (20 + 4 * (size_t)ds) + 3 * n2 + 16 * (size_t)n + 512;
+  if (b.pool.resize(need) != cudaSuccess || b.ibuf.resize(16 + 2 * (size_t)n) != cudaSuccess)
+    return dss_fail(ctx, DSS_ERR_OOM, "dss_uhf_solve: device allocation failed");
+  double* base = b.pool.ptr;
+  double *H = base, *S = H + n2, *X = S + n2, *Jt = X + n2, *T1 = Jt + n2, *T2 = T1 + n2, *Fn = T2 + n2;
+  double* Jacc[2] = {Fn + n2, Fn + 2 * n2};
+  double* Kacc[2] = {Fn + 3 * n2, Fn + 4 * n2};
+  double* D[2] = {Fn + 5 * n2, Fn + 6 * n2};
+  double* G[2] = {Fn + 7 * n2, Fn + 8 * n2};
+  double* F[2] = {Fn + 9 * n2, Fn + 10 * n2};
+  double* Cp[2] = {Fn + 11 * n2, Fn + 12 * n2};
+  double* C = Fn + 13 * n2;
+  double* Fring[2] = {C + n2, C + n2 + (size_t)ds * n2};
+  double* Ering[2] = {C + n2 + 2 * (size_t)ds * n2, C + n2 + 3 * (size_t)ds * n2};
+  double* work = C + n2 + 4 * (size_t)ds * n2;  // 3 n^2 + 64 + n ints
+  double* eps[2] = {work + 3 * n2 + 64 + (size_t)n, work + 3 * n2 + 64 + 2 * (size_t)n};
+  double* small = eps[1] + n;  // [0] E, [1..2] traces, [2..11]/[16..35] per-spin dots/coef below
+  double* dots[2] = {small + 64, small + 80};
+  double* coef[2] = {small + 96, small + 112};
+  double* Bm[2] = {small + 128, small + 228};
+  int* state[2] = {b.ibuf.ptr, b.ibuf.ptr + 8};
+  const int nocc[2] = {n_alpha, n_beta};
+  auto fail_cuda = [&](cudaError_t e, const char* what) {
+    return dss_fail(ctx, DSS_ERR_CUDA, std::string("dss_uhf_solve: ") + what + ": " + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+#define UHF_CHECK(call, what)                        \
+  do {                                               \
+    e = (call);                                      \
+    if (e != cudaSuccess) return fail_cuda(e, what); \
+  } while (0)
+  DevBuf<double> packed;
+  UHF_CHECK(packed.resize(np), "alloc");
+  UHF_CHECK(cudaMemcpyAsync(packed.ptr, Hp, np * 8, cudaMemcpyHostToDevice, s), "H2D H");
+  unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, H, n);
+  UHF_CHECK(cudaMemcpyAsync(packed.ptr, Sp, np * 8, cudaMemcpyHostToDevice, s), "H2D S");
+  unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, S, n);
+  // X = U s^-1/2 U^T (assignOrthogonalization).
+  UHF_CHECK(cudaMemcpyAsync(T1, S, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy S");
+  UHF_CHECK(dss_jacobi_eigh(s, n, T1, T2, eps[0], work, 60, DSS_JACOBI_TOL, false), "eigh(S)");
+  scale_cols<<<nb(n2), 256, 0, s>>>(T2, eps[0], T1, n, 1);
+  dss_gemm(s, n, false, true, 1.0, T1, T2, 0.0, X);
+  for (int sp = 0; sp < 2; ++sp) {
+    if (o.use_guess) {
+      UHF_CHECK(cudaMemcpyAsync(packed.ptr, sp ? Dbp : Dap, np * 8, cudaMemcpyHostToDevice, s), "H2D D");
+      unpack_sym<<<nb(n2), 256, 0, s>>>(packed.ptr, D[sp], n);
+    } else {
+      UHF_CHECK(cudaMemsetAsync(D[sp], 0, n2 * 8, s), "zero D");  // useCoreGuess, SCFSolver.cpp:179-194
+    }
+    UHF_CHECK(cudaMemsetAsync(Bm[sp], 0, 100 * 8, s), "zero B");
+  }
+  UHF_CHECK(cudaMemsetAsync(b.ibuf.ptr, 0, 16 * sizeof(int), s), "zero state");
+  BuildMode mode;
+  mode.boys = ctx->opts.boys_mode;
+  // J and K of both spin densities, combined into G_a, G_b (and J).
+  auto two_electron = [&]() -> int {
+    for (int sp = 0; sp < 2; ++sp) {
+      int r = dss_enqueue_jk(ctx, D[sp], Jacc[sp], Kacc[sp], nullptr, &mode);
+      if (r != DSS_OK) return r;
+    }
+    uhf_combine<<<nb(n2), 256, 0, s>>>(Jacc[0], Kacc[0], Jacc[1], Kacc[1], G[0], G[1], Jt, n);
+    return DSS_OK;
+  };
+  bool have_cp[2] = {false, false};
+  double E = 0.0, E_prev = 0.0;
+  int it = 0;
+  int rc = DSS_OK;
+  while (true) {
+    if (it && std::fabs(E - E_prev) < o.conv) break;
+    if (it >= o.max_iter) {
+      rc = dss_fail(ctx, DSS_ERR_NOCONV, "dss_uhf_solve: no convergence within max_iter iterations");
+      break;
+    }
+    ++it;
+    int r2 = two_electron();
+    if (r2 != DSS_OK) return r2;
+    for (int sp = 0; sp < 2; ++sp) {
+      // F_new = H + G_s; DIIS per spin (solvers[spin], SCFDIIS.cpp:14-52).
+      axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 1.0, H, 1.0, G[sp], 0.0, nullptr, Fn);
+      if (it == 1) {
+        UHF_CHECK(cudaMemcpyAsync(F[sp], Fn, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy F");
+      } else {
+        dss_gemm(s, n, false, false, 1.0, D[sp], Fn, 0.0, T1);
+        dss_gemm(s, n, false, false, 1.0, S, T1, 0.0, T2);
+        diis_choose<<<1, 1, 0, s>>>(state[sp], Bm[sp], ds, 10);
+        antisym<<<nb(n2), 256, 0, s>>>(T2, T1, n);
+        copy_slot<<<nb(n2), 256, 0, s>>>((int)n2, T1, Ering[sp], state[sp]);
+        copy_slot<<<nb(n2), 256, 0, s>>>((int)n2, Fn, Fring[sp], state[sp]);
+        UHF_CHECK(cudaMemsetAsync(dots[sp], 0, 10 * 8, s), "zero dots");
+        ring_dots<<<dim3(64, ds), 256, 0, s>>>((int)n2, Ering[sp], state[sp], dots[sp]);
+        diis_solve<<<1, 1, 0, s>>>(state[sp], Bm[sp], 10, dots[sp], coef[sp]);
+        diis_combine<<<nb(n2), 256, 0, s>>>((int)n2, Fring[sp], coef[sp], state[sp], F[sp]);
+      }
+    }
+    for (int sp = 0; sp < 2; ++sp) {
+      // F' = X F X, eigen-decomposition (warm start from the previous C'), C = X C'.
+      dss_gemm(s, n, false, false, 1.0, F[sp], X, 0.0, T1);
+      dss_gemm(s, n, false, false, 1.0, X, T1, 0.0, T2);
+      if (have_cp[sp]) {
+        dss_gemm(s, n, false, false, 1.0, T2, Cp[sp], 0.0, T1);
+        dss_gemm(s, n, true, false, 1.0, Cp[sp], T1, 0.0, T2);
+        UHF_CHECK(dss_jacobi_eigh(s, n, T2, T1, eps[sp], work, 40, DSS_JACOBI_TOL, false), "eigh(F')");
+        dss_gemm(s, n, false, false, 1.0, Cp[sp], T1, 0.0, T2);
+        UHF_CHECK(cudaMemcpyAsync(Cp[sp], T2, n2 * 8, cudaMemcpyDeviceToDevice, s), "copy C'");
+      } else {
+        UHF_CHECK(dss_jacobi_eigh(s, n, T2, Cp[sp], eps[sp], work, 60, DSS_JACOBI_TOL, false), "eigh(F')");
+        have_cp[sp] = true;
+      }
+      dss_gemm(s, n, false, false, 1.0, X, Cp[sp], 0.0, C);
+      density_kernel<<<nb(n2), 256, 0, s>>>(C, D[sp], n, nocc[sp]);
+    }
+    UHF_CHECK(cudaMemsetAsync(small + 1, 0, 16, s), "zero tr");
+    dot_kernel<<<64, 256, 0, s>>>((long long)n2, D[0], G[0], small + 1);
+    dot_kernel<<<64, 256, 0, s>>>((long long)n2, D[1], G[1], small + 2);
+    uhf_energy_kernel<<<1, 1, 0, s>>>(eps[0], n_alpha, eps[1], n_beta, small + 1, small);
+    UHF_CHECK(cudaGetLastError(), "launch");
+    double Eh = 0.0;
+    UHF_CHECK(cudaMemcpyAsync(&Eh, small, 8, cudaMemcpyDeviceToHost, s), "D2H E");
+    UHF_CHECK(cudaStreamSynchronize(s), "sync");
+    E_prev = E;
+    E = Eh;
+    if (!std::isfinite(E)) {
+      rc = dss_fail(ctx, DSS_ERR_NOCONV, "dss_uhf_solve: energy is not finite");
+      break;
+    }
+  }
+  // Final energy from the final densities (calculateEnergies, Energy.cpp:21-50):
+  // tr(Dt H) + tr(Dt J)/2 - (tr(Da Ka) + tr(Db Kb))/2 + E_nuc, Dt = Da + Db.
+  int r3 = two_electron();
+  if (r3 != DSS_OK) return r3;
+  axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 1.0, D[0], 1.0, D[1], 0.0, nullptr, T1);  // Dt
+  UHF_CHECK(cudaMemsetAsync(small + 1, 0, 40, s), "zero tr");
+  dot_kernel<<<64, 256, 0, s>>>((long long)n2, T1, H, small + 1);
+  dot_kernel<<<64, 256, 0, s>>>((long long)n2, T1, Jt, small + 2);
+  dot_kernel<<<64, 256, 0, s>>>((long long)n2, D[0], G[0], small + 3);  // tr(Da (J - Ka))
+  dot_kernel<<<64, 256, 0, s>>>((long long)n2, D[1], G[1], small + 4);
+  double tr[4];
+  UHF_CHECK(cudaMemcpyAsync(tr, small + 1, 32, cudaMemcpyDeviceToHost, s), "D2H tr");
+  for (int sp = 0; sp < 2; ++sp) {
+    double* out = sp ? Dbp : Dap;
+    if (!out) continue;
+    pack_sym<<<nb(n2), 256, 0, s>>>(D[sp], packed.ptr, n);
+    UHF_CHECK(cudaMemcpyAsync(out, packed.ptr, np * 8, cudaMemcpyDeviceToHost, s), "D2H D");
+    UHF_CHECK(cudaStreamSynchronize(s), "sync");
+  }
+  UHF_CHECK(cudaStreamSynchronize(s), "sync");
+  // tr(Ds Gs) = tr(Ds J) - tr(Ds Ks); summed over the spins: tr(Dt J) - sum tr(Ds Ks).
+  const double exch = tr[1] - (tr[2] + tr[3]);  // sum_s tr(Ds Ks)
+  *E_total = tr[0] + 0.5 * tr[1] - 0.5 * exch + e_nuc;
+  if (iterations) *iterations = it;
+#undef UHF_CHECK
   return rc;
 }
 

@@ -186,6 +186,29 @@ class FockBuilder:
             self._check(rc)
         return E.value, D, it.value, rc
 
+    def uhf(self, H: np.ndarray, S: np.ndarray, n_alpha: int, n_beta: int, e_nuc: float, conv: float = 1e-8,
+            diis_size: int = 8, max_iter: int = 128, guess: Optional[Tuple[np.ndarray, np.ndarray]] = None,
+            raise_on_noconv: bool = True):
+        """Device UHF (the unrestricted branch of scf::solveMOs).  Returns
+        (E_total, D_alpha, D_beta (packed-U), iterations, status)."""
+        n = self.nbf
+        np_ = n * (n + 1) // 2
+        o = _lib.DssScfOpts(conv, diis_size, max_iter, 1 if guess is not None else 0, 0, 1e-7, 1e-12, 8, 1e-5)
+        if guess is not None:
+            Da = np.ascontiguousarray(guess[0], dtype=np.float64).copy()
+            Db = np.ascontiguousarray(guess[1], dtype=np.float64).copy()
+        else:
+            Da, Db = np.zeros(np_), np.zeros(np_)
+        E = ctypes.c_double()
+        it = ctypes.c_int()
+        Hc = np.ascontiguousarray(H, dtype=np.float64)
+        Sc = np.ascontiguousarray(S, dtype=np.float64)
+        rc = self._L.dss_uhf_solve(self._h, _dp(Hc), _dp(Sc), int(n_alpha), int(n_beta), float(e_nuc),
+                                   ctypes.byref(o), ctypes.byref(E), _dp(Da), _dp(Db), ctypes.byref(it))
+        if rc != 0 and (raise_on_noconv or rc != -4):
+            self._check(rc)
+        return E.value, Da, Db, it.value, rc
+
     def sync(self) -> None:
         self._check(self._L.dss_sync(self._h))
 

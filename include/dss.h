@@ -162,7 +162,7 @@ int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops);
  * xyz_bohr[3*natom]), packed-U: overlap S, kinetic T and nuclear attraction V
  * (H = T + V), and the nuclear repulsion energy.  Replaces
  * scf::assignOverlapMatrix / assignCoreHamiltonian (chem/scf/SCFBasis.cpp:56-83).
- * Any output may be NULL.  Host computation, threaded over shell pairs. */
+ * Any output may be NULL.  Computed on the device (one warp per shell pair). */
 int dss_one_electron(dss_ctx* ctx, int natom, const int* Z, const double* xyz_bohr, double* S_packed,
                      double* T_packed, double* V_packed, double* e_nuc);
 
@@ -200,6 +200,20 @@ void dss_default_scf_opts(dss_scf_opts* opts);
  * Returns DSS_ERR_NOCONV when max_iter is reached (outputs still written). */
 int dss_scf_solve(dss_ctx* ctx, const double* H_packed, const double* S_packed, int n_alpha, double e_nuc,
                   const dss_scf_opts* opts, double* E_total, double* D_alpha_inout, int* iterations);
+
+/* Open-shell UHF on the device for the current basis (multiplicity > 1 in
+ * scf::assignMolecule, chem/scf/SCFBasis.cpp:17-37), replacing the
+ * unrestricted branch of scf::solveMOs + scf::calculateEnergies
+ * (chem/scf/SCFSolver.cpp:120-172,196-237; chem/scf/Energy.cpp:21-50):
+ * G_s = J[D_a + D_b] - K[D_s] from two J/K builds per iteration, one Pulay DIIS
+ * ring per spin (chem/scf/SCFDIIS.cpp:14-52), one eigensolve per spin,
+ * E_elec = sum eps_a + sum eps_b - (tr(D_a G_a) + tr(D_b G_b))/2.  n_alpha and
+ * n_beta occupied orbitals (electron_count[0], electron_count[1]).  Plain FP64
+ * form only (opts->incremental must be 0).  D_alpha_inout / D_beta_inout: the
+ * guess when opts->use_guess, and the final spin densities (packed-U). */
+int dss_uhf_solve(dss_ctx* ctx, const double* H_packed, const double* S_packed, int n_alpha, int n_beta,
+                  double e_nuc, const dss_scf_opts* opts, double* E_total, double* D_alpha_inout,
+                  double* D_beta_inout, int* iterations);
 
 /* ---------------------------------------------------------------- batches of molecules */
 /* Many closed-shell molecules of uneven size solved together: each ERI class

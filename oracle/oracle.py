@@ -265,3 +265,82 @@ def scf_rhf(S: np.ndarray, H: np.ndarray, eri: np.ndarray, n_alpha: int, e_nuc: 
     J, K = jk(eri, D)
     E_tot = 2.0 * float(np.sum(D * H)) + float(np.sum(D * J)) - float(np.sum(D * K)) + e_nuc
     return E_tot, D, it
+
+
+def _diis_ring(B, errs, focks, e, Fnew, diis_size):
+    """One Pulay DIIS step of lalib/DIIS.ipp:19-100 (ring, bordered B, dspsv);
+    returns the extrapolated Fock matrix."""
+    rms = float(np.sum(e * e))
+    if len(errs) < diis_size:
+        idx = len(errs)
+        errs.append(e)
+        focks.append(Fnew)
+    else:
+        idx = int(np.argmax([B[i, i] for i in range(diis_size)]))
+        errs[idx] = e
+        focks[idx] = Fnew
+    cnt = len(errs)
+    B[idx, idx] = rms
+    for i in range(cnt):
+        if i != idx:
+            B[i, idx] = B[idx, i] = float(np.sum(errs[i] * e))
+    if cnt <= 1:
+        return focks[0]
+    M = np.zeros((cnt + 1, cnt + 1))
+    M[:cnt, :cnt] = B[:cnt, :cnt]
+    M[:cnt, cnt] = M[cnt, :cnt] = 1.0
+    rhs = np.zeros(cnt + 1)
+    rhs[cnt] = 1.0
+    _, _, c, info = lapack.dsysv(M, rhs, lower=0)
+    if info > 0:
+        c = rhs
+    return sum(c[i] * focks[i] for i in range(cnt))
+
+
+def scf_uhf(S: np.ndarray, H: np.ndarray, eri: np.ndarray, n_alpha: int, n_beta: int, e_nuc: float,
+            conv: float = 1e-10, diis_size: int = 8, max_iter: int = 500):
+    """The reference's unrestricted loop restated (chem/scf/SCFSolver.cpp:120-172,
+    196-237; one DIIS solver per spin, chem/scf/SCFDIIS.cpp:14-52; final energy
+    chem/scf/Energy.cpp:21-50).  Returns (E_total, D_alpha, D_beta, iterations)."""
+    n = S.shape[0]
+    s, U = np.linalg.eigh(S)
+    X = (U * (1.0 / np.sqrt(s))) @ U.T
+    D = [np.zeros((n, n)), np.zeros((n, n))]
+    nocc = (n_alpha, n_beta)
+    E = 0.0
+    E_prev = 0.0
+    it = 0
+    rings = [([], [], np.zeros((diis_size + 1, diis_size + 1))) for _ in range(2)]
+    while True:
+        if it and abs(E - E_prev) < conv:
+            break
+        if it >= max_iter:
+            raise RuntimeError("oracle UHF did not converge")
+        it += 1
+        Dt = D[0] + D[1]
+        J = np.einsum("mnst,st->mn", eri, Dt)
+        G = [J - np.einsum("mtsn,st->mn", eri, D[sp]) for sp in range(2)]
+        F = []
+        for sp in range(2):
+            Fnew = H + G[sp]
+            if it == 1:
+                F.append(Fnew)
+            else:
+                spf = S @ (D[sp] @ Fnew)
+                errs, focks, B = rings[sp]
+                F.append(_diis_ring(B, errs, focks, spf - spf.T, Fnew, diis_size))
+        eps = []
+        for sp in range(2):
+            e_s, Cp = np.linalg.eigh(X @ F[sp] @ X)
+            C = X @ Cp
+            D[sp] = C[:, :nocc[sp]] @ C[:, :nocc[sp]].T
+            eps.append(e_s)
+        E_prev = E
+        E = (float(np.sum(eps[0][:n_alpha])) + float(np.sum(eps[1][:n_beta]))
+             - 0.5 * float(np.sum(D[0] * G[0])) - 0.5 * float(np.sum(D[1] * G[1])))
+    Dt = D[0] + D[1]
+    J = np.einsum("mnst,st->mn", eri, Dt)
+    Ks = [np.einsum("mtsn,st->mn", eri, D[sp]) for sp in range(2)]
+    E_tot = (float(np.sum(Dt * H)) + 0.5 * float(np.sum(Dt * J))
+             - 0.5 * float(np.sum(D[0] * Ks[0])) - 0.5 * float(np.sum(D[1] * Ks[1])) + e_nuc)
+    return E_tot, D[0], D[1], it

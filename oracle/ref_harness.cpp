@@ -210,8 +210,9 @@ int ref_basis_prims(int f, double* zeta, double* weight) {
   return (int)g.primitives.size();
 }
 
-// RHF SCF from the core guess to |dE| < conv.  Returns the iteration count;
-// fills E_total and the final alpha density (packed-U).
+// SCF from the core guess to |dE| < conv (RHF, or UHF when ref_setup had
+// multiplicity > 1).  Returns the iteration count; fills E_total and the final
+// alpha density (packed-U).
 int ref_scf(double conv, double* E_total, double* D_alpha_packed, double* seconds, int quiet) {
   if (!g_have_tensor) return -1;
   if (quiet) quiet_on();
@@ -225,6 +226,14 @@ int ref_scf(double conv, double* E_total, double* D_alpha_packed, double* second
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   if (quiet) quiet_off();
   return (int)scf::iteration;
+}
+
+// Spin density (0 = alpha, 1 = beta; packed-U) after ref_scf, and the
+// electron counts scf::assignMolecule derived from charge and multiplicity.
+void ref_get_density(int spin, double* D_packed) { copy_packed(scf::density_matrix[spin ? 1 : 0], D_packed); }
+void ref_electron_counts(int* n_alpha, int* n_beta) {
+  *n_alpha = (int)scf::electron_count[0];
+  *n_beta = (int)scf::electron_count[1];
 }
 
 // Two-electron Fock part for a given alpha density: G = J[2 D_alpha] - K[D_alpha]

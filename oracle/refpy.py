@@ -41,6 +41,8 @@ def lib():
         L.ref_basis_prims.restype = ctypes.c_int
         L.ref_scf.argtypes = [ctypes.c_double, dp, dp, dp, ctypes.c_int]
         L.ref_scf.restype = ctypes.c_int
+        L.ref_get_density.argtypes = [ctypes.c_int, dp]
+        L.ref_electron_counts.argtypes = [ip, ip]
         L.ref_fock_2e.argtypes = [dp, dp]
         L.ref_fock_2e.restype = ctypes.c_int
         L.ref_jk.argtypes = [dp, dp, dp]
@@ -88,6 +90,21 @@ def scf(conv: float = 1e-10) -> Tuple[float, np.ndarray, int, float]:
     if it < 0:
         raise RuntimeError("reference state has no ERI tensor")
     return E.value, D, it, secs.value
+
+
+def spin_density(spin: int) -> np.ndarray:
+    """Final alpha (0) or beta (1) density of the last scf() call, packed-U."""
+    L = lib()
+    n = L.ref_nbf()
+    D = np.zeros(n * (n + 1) // 2)
+    L.ref_get_density(int(spin), _p(D))
+    return D
+
+
+def electron_counts() -> Tuple[int, int]:
+    a, b = ctypes.c_int(), ctypes.c_int()
+    lib().ref_electron_counts(ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
 
 
 def fock_2e(D_alpha_packed: np.ndarray) -> np.ndarray:

@@ -7,6 +7,9 @@ oracle/build_ref.sh and driven through oracle/ref_harness.cpp:
                    energy (|dE| < 1e-10), the final alpha density (packed-U),
                    J[D_total], K[D_alpha] and G = J - K at that density, the
                    same three for a seeded random symmetric density, S and H.
+  * <name>_uhf.npz open-shell molecules (multiplicity > 1, the reference's
+                   unrestricted branch): charge, multiplicity, electron counts,
+                   the converged energy and both final spin densities, S and H.
 
 Usage (in a container with /root/reference): python tests/golden/make_golden.py [case ...]
 (with case names: only those fixtures; (H2O)8 takes several minutes)
@@ -48,6 +51,39 @@ def cases():
     return out
 
 
+def uhf_cases():
+    """Open-shell molecules (name, molecule, basis, 5D, charge, multiplicity).  All of
+    them converge without a singular DIIS system in the reference; radicals whose
+    beta HOMO is degenerate (OH) or whose DIIS wanders for hundreds of iterations
+    (CH3, NH2 in STO-3G) make the converged state depend on rounding and are left out."""
+    A = basis.molecule_from_angstrom
+    ch2 = [[0, 0, 0], [0.9918, 0.4226, 0], [-0.9918, 0.4226, 0]]
+    return [
+        ("ch2_631gs_uhf", A(["C", "H", "H"], ch2), "6-31G*", True, 0, 3),
+        ("ch2_631g_uhf", A(["C", "H", "H"], ch2), "6-31G", True, 0, 3),
+        ("nh2_631g_uhf", A(["N", "H", "H"], [[0, 0, 0], [0.80, 0.63, 0], [-0.80, 0.63, 0]]), "6-31G", True, 0, 2),
+        ("h2op_631g_uhf", geometry.water(), "6-31G", True, 1, 2),
+        ("li_631g_uhf", A(["Li"], [[0, 0, 0]]), "6-31G", True, 0, 2),
+        ("beh_631g_uhf", A(["Be", "H"], [[0, 0, 0], [0, 0, 1.343]]), "6-31G", True, 0, 2),
+        ("hco_sto3g_uhf", A(["H", "C", "O"], [[-0.9, 0.75, 0], [0, 0, 0], [1.18, 0, 0]]), "STO-3G", True, 0, 2),
+        ("c2h3_sto3g_uhf", A(["C", "C", "H", "H", "H"], [[0, 0, 0], [1.31, 0, 0], [-0.55, 0.93, 0], [-0.55, -0.93, 0],
+                                                       [1.9, 0.9, 0]]), "STO-3G", True, 0, 2),
+    ]
+
+
+def write_uhf_case(name, mol, bas, pure, charge, mult) -> None:
+    sh = shells.build_shells(mol, basis.builtin_basis(bas), pure=pure)
+    n = refpy.setup(sh, charge=charge, multiplicity=mult)
+    E, Da, it, secs = refpy.scf(1e-10)
+    Db = refpy.spin_density(1)
+    na, nb = refpy.electron_counts()
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"), Z=np.asarray(mol.Z), xyz=np.asarray(mol.xyz), basis=bas,
+        pure=pure, charge=charge, multiplicity=mult, n_alpha=na, n_beta=nb, nbf=n, E=E, iterations=it,
+        Da=Da, Db=Db, S=refpy.overlap(), H=refpy.core_hamiltonian(), e_nuc=mol.nuclear_repulsion())
+    print(f"{name:18s} n={n:4d} na={na} nb={nb} E={E:.13f} it={it} ({secs:.2f}s)")
+
+
 def main() -> None:
     only = set(sys.argv[1:])
     if only:
@@ -55,6 +91,9 @@ def main() -> None:
         for name, mol, bas, pure in cases():
             if name in only:
                 write_case(name, mol, bas, pure, rng)
+        for name, mol, bas, pure, charge, mult in uhf_cases():
+            if name in only:
+                write_uhf_case(name, mol, bas, pure, charge, mult)
         return
     xs = np.concatenate([[0.0, 1e-12, 1e-9, 1e-6, 1e-3], np.linspace(0.01, 40.0, 397), [24.99, 25.0, 25.01, 26.1, 26.2]])
     ms = np.arange(0, 13)
@@ -63,6 +102,8 @@ def main() -> None:
     rng = np.random.default_rng(1234)
     for name, mol, bas, pure in cases():
         write_case(name, mol, bas, pure, rng)
+    for name, mol, bas, pure, charge, mult in uhf_cases():
+        write_uhf_case(name, mol, bas, pure, charge, mult)
 
 
 def write_case(name, mol, bas, pure, rng) -> None:

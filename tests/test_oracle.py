@@ -100,6 +100,27 @@ def test_oracle_scf_matches_reference_energy(name):
     assert abs(E - float(d["E"])) < 1e-9
 
 
+UHF_CASES = ["ch2_631gs_uhf", "ch2_631g_uhf", "nh2_631g_uhf", "h2op_631g_uhf", "li_631g_uhf", "beh_631g_uhf",
+             "hco_sto3g_uhf", "c2h3_sto3g_uhf"]
+
+
+@pytest.mark.parametrize("name", UHF_CASES)
+def test_oracle_uhf_matches_reference_energy(name):
+    d, mol, sh = load_case(name)
+    n = int(d["nbf"])
+    eri = oracle.eri_tensor(sh)
+    S = shells.unpack(d["S"], n)
+    H = shells.unpack(d["H"], n)
+    E, Da, Db, it = oracle.scf_uhf(S, H, eri, int(d["n_alpha"]), int(d["n_beta"]), float(d["e_nuc"]), max_iter=2000)
+    assert abs(E - float(d["E"])) < 1e-9
+    # Electron counts tr(D_s S).  The densities themselves are not compared: where
+    # occupied orbitals are (near-)degenerate the converged spin densities differ by
+    # a rotation of equal energy between any two eigensolvers.
+    assert abs(np.sum(Da * S) - int(d["n_alpha"])) < 1e-8
+    assert abs(np.sum(Db * S) - int(d["n_beta"])) < 1e-8
+    assert abs(np.sum(shells.unpack(d["Da"], n) * S) - int(d["n_alpha"])) < 1e-8
+
+
 @pytest.mark.skipif(not refpy.available(), reason="oracle/_ref not built")
 def test_oracle_eri_matches_live_reference():
     d, mol, sh = load_case("water_631gs_6d")
