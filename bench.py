@@ -59,6 +59,92 @@ def _dist_env():
     return ws, rank, local
 
 
+def _radical(mol):
+    """The molecule without its last hydrogen (an alkyl radical from an alkane)."""
+    from dollarstorescf_b200.basis import Molecule
+
+    k = max(i for i, z in enumerate(mol.Z) if z == 1)
+    return Molecule([z for i, z in enumerate(mol.Z) if i != k], [p for i, p in enumerate(mol.xyz) if i != k])
+
+
+def measure_rows(device: int, cpu_baseline: bool):
+    """The rows next to the Fock build: device one-electron integrals and device
+    UHF, each beside the reference's own CPU code on the same input (one host
+    core, the reference is single-threaded).
+
+      one_electron  (H2O)32 6-31G* 6D (608 functions, 96 nuclei): dss_one_electron
+                    (S, T, V to host) vs the reference's basis set-up without the
+                    ERI tensor (S, T, V and the Loewdin X).
+      uhf           CH2 triplet 6-31G* and the n-butyl radical 6-31G (doublet):
+                    dss_uhf_solve from the core guess, conv 1e-10, vs the
+                    reference's unrestricted solveMOs (ERI tensor + SCF).
+    """
+    import time as _t
+
+    from dollarstorescf_b200 import basis as B
+    from dollarstorescf_b200 import geometry, shells
+    from dollarstorescf_b200.engine import BOYS_REF, FockBuilder
+
+    out = {}
+    w32 = geometry.water_cluster(4, 4, 2, 32, seed=2024)
+    sh32 = shells.build_shells(w32, B.builtin_basis("6-31G*"), pure=False)
+    with FockBuilder(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as fb:
+        fb.set_basis(sh32)
+        fb.one_electron(sh32)
+        ts = []
+        for _ in range(5):
+            t0 = _t.perf_counter()
+            fb.one_electron(sh32)
+            ts.append(_t.perf_counter() - t0)
+    ts.sort()
+    oe = {"workload": "(H2O)32 6-31G* 6D S, T, V (608 functions, 96 nuclei)", "gpu_ms": ts[2] * 1e3,
+          "per_s": 1.0 / ts[2]}
+    if cpu_baseline:
+        from oracle import refpy
+
+        if refpy.available():
+            t0 = _t.perf_counter()
+            refpy.setup(sh32, build_tensor=False)
+            dt = _t.perf_counter() - t0
+            oe["cpu_baseline"] = {"seconds": dt, "per_s": 1.0 / dt, "cores": 1, "kind": "reference",
+                                  "sample": "the reference's basis set-up without the ERI tensor (S, T, V, X)"}
+            oe["gpu_over_cpu"] = dt / ts[2]
+    out["one_electron"] = oe
+
+    A = B.molecule_from_angstrom
+    cases = [("ch2_631gs_triplet", A(["C", "H", "H"], [[0, 0, 0], [0.9918, 0.4226, 0], [-0.9918, 0.4226, 0]]),
+              "6-31G*", 3),
+             ("c4h9_631g_doublet", _radical(geometry.alkane(4, 0)), "6-31G", 2)]
+    uhf = {}
+    for name, mol, bas, mult in cases:
+        sh = shells.build_shells(mol, B.builtin_basis(bas), pure=True)
+        ne = sh.n_electrons()
+        na, nb = (ne + mult) // 2, (ne + 1 - mult) // 2
+        r = {"nbf": sh.nbf(), "n_alpha": na, "n_beta": nb}
+        with FockBuilder(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as fb:
+            fb.set_basis(sh)
+            t0 = _t.perf_counter()
+            S, T, V, en = fb.one_electron(sh)
+            E, Da, Db, it, rc = fb.uhf(T + V, S, na, nb, en, conv=1e-10, max_iter=1000, raise_on_noconv=False)
+            dt = _t.perf_counter() - t0
+        r["gpu"] = {"solves_per_s": 1.0 / dt, "iterations": it, "energy": E, "status": rc}
+        if cpu_baseline:
+            from oracle import refpy
+
+            if refpy.available():
+                t0 = _t.perf_counter()
+                refpy.setup(sh, charge=0, multiplicity=mult)
+                Er, _, itr, _ = refpy.scf(1e-10)
+                dtr = _t.perf_counter() - t0
+                r["cpu_baseline"] = {"solves_per_s": 1.0 / dtr, "iterations": itr, "energy": Er, "cores": 1,
+                                     "kind": "reference", "sample": "one full unrestricted solve (ERI tensor + SCF)"}
+                r["abs_dE_vs_reference"] = abs(E - Er)
+                r["gpu_over_cpu"] = dtr / dt
+        uhf[name] = r
+    out["uhf"] = uhf
+    return out
+
+
 # ---------------------------------------------------------------- reference arm
 def _ref_worker(args):
     seconds_budget, seed = args
@@ -363,6 +449,7 @@ def run_gpu(args):
     fb.close()
     if rank == 0 and not args.no_forms:
         line["forms"] = measure_forms(device, args.forms_molecules, args.forms_requests)
+        line["forms"].update(measure_rows(device, cpu_baseline=not args.no_cpu_baseline))
     if rank == 0:
         print(json.dumps(line))
     if ws > 1:

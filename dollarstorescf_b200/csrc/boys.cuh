@@ -293,13 +293,14 @@ __device__ __forceinline__ void boys_ref_walk(double x, double* F) {
 }
 
 // Reference-mode Boys from the cell records (cells = the library's copy of
-// g_boys_cell, boys_cell_data.cu, passed in the kernel arguments): one
-// record per order m and grid point k = round(16 x) holds the Taylor
-// coefficients, about k/16, of the reference's value on both sides of the one
-// truncation breakpoint b the cell may contain (b = 1e300 when it has none).
-// The asymptotic form is evaluated for every lane (one rsqrt); a lane reads the
-// record of order m only when x <= 1.1 m + 25, picks the half by x > b and
-// evaluates it: no search, two dependent loads, seven FMAs per order.  The
+// g_boys_cell, boys_cell_data.cu, passed in the kernel arguments): per order m
+// and grid point k = round(16 x) a 64-byte record holds the Taylor
+// coefficients, about k/16, of the reference's value up to the one truncation
+// breakpoint b the cell may contain (b = 1e300 when it has none) and b itself;
+// a second record at the same index of block B holds the piece past b.
+// Orders with x > 1.1 m + 25 take the asymptotic form (one rsqrt for all of
+// them); every other order reads its A record (four 16-byte loads, b included),
+// the B record only when x > b, and evaluates seven FMAs: no search.  The
 // series itself (a separate function) runs only for x < 1/32 (cell 0 holds
 // several breakpoints) and within 4e-14 (relative) of a breakpoint, where the
 // rounding of the reference's own sum decides its stop.
@@ -334,10 +335,16 @@ __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
     if (m < m_lo) continue;
-    const double2* r = reinterpret_cast<const double2*>(cells) + ((size_t)m * DSS_BOYS_NCELL + k) * 8;
-    const double b = __ldg(&r[3].y);
-    const double2* c = r + (x > b ? 4 : 0);
-    const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c6b = __ldg(c + 3);
+    const double2* r = reinterpret_cast<const double2*>(cells) + ((size_t)m * DSS_BOYS_NCELL + k) * 4;
+    double2 c01 = __ldg(r), c23 = __ldg(r + 1), c45 = __ldg(r + 2), c6b = __ldg(r + 3);
+    const double b = c6b.y;
+    if (x > b) {  // the piece past the cell's breakpoint, same index in block B
+      r += (size_t)DSS_BOYS_NMC * DSS_BOYS_NCELL * 4;
+      c01 = __ldg(r);
+      c23 = __ldg(r + 1);
+      c45 = __ldg(r + 2);
+      c6b = __ldg(r + 3);
+    }
     double f = c6b.x;
     f = f * dx + c45.y;
     f = f * dx + c45.x;

@@ -103,26 +103,29 @@ def main() -> None:
     def nidx(m, x):
         return 1 + sum(1 for k in range(1, NB + 1) if BP[m][k] < x)
 
-    # One 128-byte record per order m and grid point k (cell
+    # Two 64-byte records per order m and grid point k (cell
     # [k/16 - 1/32, k/16 + 1/32]).  Away from x = 0 a cell holds at most one
     # truncation breakpoint b (checked below, with a margin), so the
     # reference's value in the cell is G_{m,nA} for x <= b and G_{m,nA+1} for
     # x > b; both are entire functions, so both expand about the cell's own node
     # x0 = k/16 with |x - x0| <= 1/32.  Record layout (doubles): [0..6] Taylor
-    # coefficients of the x <= b piece, [7] b, [8..14] those of the x > b piece,
-    # [15] b; b = 1e300 when the cell has no breakpoint (both halves then hold
-    # the same piece).  Cell 0 (x < 1/32) holds several breakpoints and is not
-    # tabulated; cells above 16 (1.1 m + 25) + 1 are not used.
+    # coefficients, [7] b.  Block A (the first NMC * NCELL records) holds the
+    # x <= b piece, block B (the next NMC * NCELL) the x > b piece at the same
+    # index; b = 1e300 when the cell has no breakpoint (its B record is never
+    # read).  A lane reads one 64-byte A record and, only when x > b, the B record.
+    # Cell 0 (x < 1/32) holds several breakpoints and is not tabulated; cells
+    # above 16 (1.1 m + 25) + 1 are not used.
     NMC = 9
     NCELL = 544
     MARGIN = 1e-9
-    CELL = []
+    CA, CB = [], []
     for m in range(NMC):
         kmax = int(round(STEP * (1.1 * m + 25))) + 1
         assert kmax < NCELL
         for k in range(NCELL):
             if k == 0 or k > kmax:
-                CELL.extend([0.0] * 7 + [1e300] + [0.0] * 7 + [1e300])
+                CA.extend([0.0] * 7 + [1e300])
+                CB.extend([0.0] * 7 + [1e300])
                 continue
             lo, hi = k / STEP - 0.5 / STEP - MARGIN, k / STEP + 0.5 / STEP + MARGIN
             bs = [BP[m][j] for j in range(1, NB + 1) if lo <= BP[m][j] <= hi]
@@ -130,11 +133,14 @@ def main() -> None:
             x0 = k / STEP
             if not bs:
                 pa = taylor(m, nidx(m, x0), x0)
-                CELL.extend(pa + [1e300] + pa + [1e300])
+                CA.extend(pa + [1e300])
+                CB.extend(pa + [1e300])
             else:
                 b = bs[0]
                 na = nidx(m, b)  # interval (B[na-1], B[na] = b]
-                CELL.extend(taylor(m, na, x0) + [b] + taylor(m, na + 1, x0) + [b])
+                CA.extend(taylor(m, na, x0) + [b])
+                CB.extend(taylor(m, na + 1, x0) + [b])
+    CELL = CA + CB
     defines += [("DSS_BOYS_NMC", NMC), ("DSS_BOYS_NCELL", NCELL)]
     tables.append(("double", "g_odd_inv", 8, [1.0 / (2 * k + 1) for k in range(256)]))
 
