@@ -106,6 +106,10 @@ def load():
     L.dss_uhf_solve.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(DssScfOpts),
                                 dp, dp, dp, ip]
     L.dss_uhf_solve.restype = ctypes.c_int
+    L.dss_scf_orbitals.argtypes = [vp, ctypes.c_int, dp, dp]
+    L.dss_scf_orbitals.restype = ctypes.c_int
+    L.dss_write_molden.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ip, dp, ctypes.c_int]
+    L.dss_write_molden.restype = ctypes.c_int
     L.dss_build_jk_device_noalloc.argtypes = [vp, vp, vp, vp]
     L.dss_build_jk_device_noalloc.restype = ctypes.c_int
     szt = ctypes.c_size_t

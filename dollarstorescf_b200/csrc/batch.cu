@@ -523,10 +523,12 @@ __global__ void k_admit_init(double* base, int n, const double* Hp, const double
   }
 }
 
-__global__ void k_scale_cols_inv_sqrt(const double* U, const double* w, double* out, int n) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)n * n) return;
-  out[t] = U[t] / sqrt(w[t % n]);
+// out = V diag(eps)^-1/2 per molecule (eps: the molecule's eigenvalue slot).
+__global__ void k_scale_cols_eps(BatchView v, int kv, int kout) {
+  BV_BEGIN();
+  const double* w = eps_of(base, n, v.ds);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+    mat(base, n, kout)[t] = mat(base, n, kv)[t] / sqrt(w[t % n]);
 }
 
 inline dim3 grid2(long long per_mol, int nb) {
@@ -545,6 +547,7 @@ struct dss_batch_mol {
   size_t size = 0;
   BasisHost basis;  // molecule-local
   PairSet pairs;    // its shell pairs and Schwarz factors, made once at admission
+  bool needs_x = true;  // X = S^-1/2 not computed yet (done for all new molecules at the next step)
 };
 
 struct dss_batch {
@@ -560,6 +563,8 @@ struct dss_batch {
   std::vector<int> slot_mol;  // batch slot -> molecule handle
   DevBuf<long long> d_region;
   DevBuf<int> d_n, d_active, d_active_next, d_nact;
+  DevBuf<int> d_pending;  // per slot: 1 while the molecule's X is not computed
+  DevBuf<double> admit_tmp;  // admission scratch (packed H, S, guess), grow-only
   int nmax = 0;
   int* h_nact = nullptr;  // pinned: molecules still iterating, molecules finished in the last iteration
   std::vector<int> last_finished;  // handles whose results the last dss_batch_step produced
@@ -719,6 +724,68 @@ bool same_opts(const dss_scf_opts& a, const dss_scf_opts& c) {
          a.rebuild_every == c.rebuild_every && a.final_switch == c.final_switch;
 }
 
+// Eigensolver, one block of 512 threads per molecule, in up to three launches
+// by size: matrix and rotations in shared memory, matrix only, neither.
+// Eigenvalues go to each molecule's eps slot, eigenvectors (columns) to kv.
+void launch_jacobi(dss_batch* b, const BatchView& v, int ka, int kv, int kt, int max_sweeps) {
+  cudaStream_t s = b->ctx->stream;
+  const int nb = (int)b->slot_mol.size();
+  static int optin = 0;
+  if (!optin) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(k_jacobi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(k_jacobi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  }
+  auto fits = [&](int nn_, bool vt) {
+    return (dss_packed_size(nn_) + (vt ? (size_t)nn_ * nn_ : 0)) * 8 + dss_block_jacobi_smem(nn_) <= (size_t)optin;
+  };
+  int n1 = 0, n2 = 0;
+  while (fits(n1 + 1, true)) ++n1;
+  while (fits(n2 + 1, false)) ++n2;
+  int top[3] = {0, 0, 0};
+  for (int k = 0; k < nb; ++k) {
+    const int nk = b->mols[b->slot_mol[k]].n;
+    const int mode = nk <= n1 ? 0 : (nk <= n2 ? 1 : 2);
+    top[mode] = std::max(top[mode], nk);
+  }
+  if (top[0])
+    k_jacobi<0><<<nb, 512, (dss_packed_size(top[0]) + (size_t)top[0] * top[0]) * 8 + dss_block_jacobi_smem(top[0]),
+                  s>>>(v, ka, kv, kt, max_sweeps, DSS_JACOBI_TOL, 0, n1);
+  if (top[1])
+    k_jacobi<1><<<nb, 512, dss_packed_size(top[1]) * 8 + dss_block_jacobi_smem(top[1]), s>>>(
+        v, ka, kv, kt, max_sweeps, DSS_JACOBI_TOL, n1, n2);
+  if (top[2])
+    k_jacobi<2><<<nb, 512, dss_block_jacobi_smem(top[2]), s>>>(v, ka, kv, kt, max_sweeps, DSS_JACOBI_TOL, n2,
+                                                               1 << 30);
+}
+
+// X = U s^-1/2 U^T (assignOrthogonalization, chem/scf/SCFBasis.cpp:85-100) for
+// every molecule admitted since the last step, all in one batched eigensolve:
+// admission stays cheap and a burst of new molecules shares the launches.
+int prepare_x(dss_batch* b) {
+  const int nb = (int)b->slot_mol.size();
+  std::vector<int> pend(nb, 0);
+  bool any = false;
+  for (int k = 0; k < nb; ++k)
+    if (b->mols[b->slot_mol[k]].needs_x) pend[k] = 1, any = true;
+  if (!any) return DSS_OK;
+  cudaStream_t s = b->ctx->stream;
+  if (b->d_pending.resize(std::max(nb, 1)) != cudaSuccess) return DSS_ERR_OOM;
+  if (cudaMemcpyAsync(b->d_pending.ptr, pend.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return DSS_ERR_CUDA;
+  BatchView v = view(b, b->d_pending.ptr);
+  const long long nn = (long long)b->nmax * b->nmax;
+  const int tiles = (b->nmax + 31) / 32;
+  launch_jacobi(b, v, M_T1, M_V, M_T3, 60);  // M_T1 holds S since admission
+  k_scale_cols_eps<<<grid2(nn, nb), 256, 0, s>>>(v, M_V, M_T2);
+  k_gemm<<<dim3(tiles, tiles, nb), dim3(32, 8), 0, s>>>(v, M_T2, M_V, M_X, 0, 1, 1.0, 0.0);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return DSS_ERR_CUDA;  // pend is freed on return
+  for (int k = 0; k < nb; ++k) b->mols[b->slot_mol[k]].needs_x = false;
+  return DSS_OK;
+}
+
 // One SCF iteration for the active molecules (the captured body).  The
 // incremental form (o.incremental) follows dss_scf_solve's: G = G_prev +
 // G[2 dD] with the density-weighted screen (FP32 quartets below fp32_threshold,
@@ -778,36 +845,7 @@ int enqueue_iteration(dss_batch* b, const dss_scf_opts& o) {
   k_gemm<<<gg, gb, 0, s>>>(v, M_X, M_T1, M_T2, 0, 0, 1.0, 0.0);
   k_gemm<<<gg, gb, 0, s>>>(v, M_T2, M_CP, M_T1, 0, 0, 1.0, 0.0);
   k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_T1, M_T2, 1, 0, 1.0, 0.0);
-  // Eigensolver, one block of 512 threads per molecule, in up to three launches
-  // by size: matrix and rotations in shared memory, matrix only, neither.
-  static int optin = 0;
-  if (!optin) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncSetAttribute(k_jacobi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    cudaFuncSetAttribute(k_jacobi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-  }
-  auto fits = [&](int nn_, bool vt) {
-    return (dss_packed_size(nn_) + (vt ? (size_t)nn_ * nn_ : 0)) * 8 + dss_block_jacobi_smem(nn_) <= (size_t)optin;
-  };
-  int n1 = 0, n2 = 0;
-  while (fits(n1 + 1, true)) ++n1;
-  while (fits(n2 + 1, false)) ++n2;
-  int top[3] = {0, 0, 0};
-  for (int k = 0; k < nb; ++k) {
-    const int nk = b->mols[b->slot_mol[k]].n;
-    const int mode = nk <= n1 ? 0 : (nk <= n2 ? 1 : 2);
-    top[mode] = std::max(top[mode], nk);
-  }
-  if (top[0])
-    k_jacobi<0><<<nb, 512, (dss_packed_size(top[0]) + (size_t)top[0] * top[0]) * 8 + dss_block_jacobi_smem(top[0]),
-                  s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL, 0, n1);
-  if (top[1])
-    k_jacobi<1><<<nb, 512, dss_packed_size(top[1]) * 8 + dss_block_jacobi_smem(top[1]), s>>>(
-        v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL, n1, n2);
-  if (top[2])
-    k_jacobi<2><<<nb, 512, dss_block_jacobi_smem(top[2]), s>>>(v, M_T2, M_V, M_T3, 40, DSS_JACOBI_TOL, n2, 1 << 30);
+  launch_jacobi(b, v, M_T2, M_V, M_T3, 40);
   // C' <- C' V (through T1), C = X C', D = C_occ C_occ^T
   k_gemm<<<gg, gb, 0, s>>>(v, M_CP, M_V, M_T1, 0, 0, 1.0, 0.0);
   k_copy<<<grid2(nn, nb), 256, 0, s>>>(v, M_T1, M_CP);
@@ -970,20 +1008,18 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   m.region = (long long)off;
   cudaStream_t s = b->ctx->stream;
   cudaSetDevice(b->ctx->opts.device);
-  DevBuf<double> tmp;
+  DevBuf<double>& tmp = b->admit_tmp;
   const int n = m.n;
   const size_t n2 = (size_t)n * n;
-  if (tmp.resize(3 * np + 4 * n2 + 128 + n) != cudaSuccess) {
+  if (tmp.resize(3 * np) != cudaSuccess) {
     arena_free(b, off, m.size);
     return bfail(b, DSS_ERR_OOM, "dss_batch_add: device allocation failed");
   }
   double* dH = tmp.ptr;
   double* dS = dH + np;
   double* dD = dS + np;
-  double* work = dD + np;  // 3 n^2 + 64 + n
-  double* w = work + 3 * n2 + 64 + n;
   // S and H = T + V straight into the scratch (device one-electron kernels).
-  rc = dss_one_electron_device(s, m.basis, natom, Z, xyz, dS, dH, nullptr, &err);
+  rc = dss_one_electron_device(s, m.basis, natom, Z, xyz, dS, dH, nullptr, &err, &b->ctx->oe_scratch);
   if (rc != DSS_OK) {
     arena_free(b, off, m.size);
     return bfail(b, rc, err);
@@ -993,17 +1029,8 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   k_admit_init<<<(unsigned)std::min<size_t>((n2 + 255) / 256, 1024), 256, 0, s>>>(base, n, dH, dS,
                                                                                   D_guess ? dD : nullptr, m.nocc,
                                                                                   e_nuc);
-  // X = U s^-1/2 U^T from the eigen-decomposition of S (assignOrthogonalization).
-  double* A = base + kHdr + (size_t)M_T1 * n2;
-  double* U = base + kHdr + (size_t)M_V * n2;
-  double* X = base + kHdr + (size_t)M_X * n2;
-  double* T2 = base + kHdr + (size_t)M_T2 * n2;
-  cudaError_t e = dss_jacobi_eigh(s, n, A, U, w, work, 60, DSS_JACOBI_TOL, false);
-  if (e == cudaSuccess) {
-    k_scale_cols_inv_sqrt<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(U, w, T2, n);
-    dss_gemm(s, n, false, true, 1.0, T2, U, 0.0, X);
-    e = cudaStreamSynchronize(s);
-  }
+  // X is computed for all new molecules together at the next dss_batch_step.
+  const cudaError_t e = cudaStreamSynchronize(s);  // the scratch is reused by the next admission
   if (e != cudaSuccess) {
     arena_free(b, off, m.size);
     return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_add: ") + cudaGetErrorString(e));
@@ -1034,6 +1061,10 @@ int dss_batch_step(dss_batch* b, const dss_scf_opts* opts, int iterations, int* 
   const int nb = (int)b->slot_mol.size();
   if (n_active) *n_active = 0;
   if (!nb) return DSS_OK;
+  {
+    const int rc = prepare_x(b);
+    if (rc != DSS_OK) return bfail(b, rc, "dss_batch_step: orthogonalisation of new molecules failed");
+  }
   if (fresh) {
     BatchView v = view(b, b->d_active.ptr);
     k_active_from_hdr<<<(nb + 127) / 128, 128, 0, s>>>(v, b->d_active.ptr, 0);

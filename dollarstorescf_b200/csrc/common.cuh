@@ -7,16 +7,17 @@
 #include "boys.cuh"
 
 // One primitive pair of a shell pair (a, b): exponent sum p = alpha + beta, 1/p,
-// the Gaussian product centre P, P - A and the pair prefactor
+// the Gaussian product centre P, P - A, the pair prefactor
 // K = w_a w_b exp(-alpha beta / p |A - B|^2), w the normalised primitive weights
-// (chem/GTO.cpp:90-93 times the file coefficient).  80 bytes, 16-byte aligned, so
-// a lane fetches one with five 16-byte loads.
+// (chem/GTO.cpp:90-93 times the file coefficient), and Kp = sqrt(2 pi^2.5) K / p,
+// the pair's share of the ERI prefactor.  80 bytes, 16-byte aligned, so a lane
+// fetches one with five 16-byte loads.
 struct __align__(16) PrimPair {
   double p, inv_p;
   double Px, Py, Pz;
   double PAx, PAy, PAz;
   double K;
-  double pad;
+  double Kp;
 };
 
 __device__ __forceinline__ PrimPair load_pp(const PrimPair* __restrict__ src) {
@@ -27,7 +28,7 @@ __device__ __forceinline__ PrimPair load_pp(const PrimPair* __restrict__ src) {
   r.Px = b.x; r.Py = b.y;
   r.Pz = c.x; r.PAx = c.y;
   r.PAy = d.x; r.PAz = d.y;
-  r.K = e.x; r.pad = e.y;
+  r.K = e.x; r.Kp = e.y;
   return r;
 }
 
@@ -61,7 +62,7 @@ __device__ __forceinline__ void prim_quartet(const PrimPair& b, const PrimPair& 
   oo2p = 0.5 * b.inv_p;
   oo2q = 0.5 * k.inv_p;
   oo2pq = 0.5 * inv_pq;
-  const double pref = DSS_TWO_PI_25 * b.K * k.K * b.inv_p * k.inv_p * r_pq;
+  const double pref = b.Kp * k.Kp * r_pq;  // 2 pi^2.5 K_ab K_cd / (p q sqrt(p+q))
   boys_eval<BOYS, L>(T, F, cells);
 #pragma unroll
   for (int m = 0; m <= L; ++m) F[m] *= pref;

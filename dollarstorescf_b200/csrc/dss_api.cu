@@ -19,6 +19,9 @@ namespace {
 thread_local std::string g_create_error;
 
 constexpr double kPiRef = 3.14159265358979;  // lalib/MathUtil.hpp:8
+// 2 pi^2.5 with the reference's PI, the ERI prefactor of chem/GaussianIntegral.cpp:632
+// (DSS_TWO_PI_25 in common.cuh).
+constexpr double kTwoPi25 = 34.98683665524963;
 
 double dfact(int n) {
   double r = 1.0;
@@ -131,6 +134,7 @@ int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* ex
                         (std::sqrt(kPiRef) * dfact(2 * l[s] + 1));
       B.exps.push_back(zeta);
       B.wts.push_back(coefs[off + p] * std::sqrt(nf));
+      B.coefs.push_back(coefs[off + p]);
     }
     off += nprim[s];
     f0 += pure ? 2 * l[s] + 1 : (l[s] + 1) * (l[s] + 2) / 2;
@@ -377,14 +381,14 @@ int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out) {
         r.PAz = r.Pz - Az;
         // chem/GaussianIntegral.cpp:583,585: exp(-alpha*beta/eta * |A-B|^2) times the weights.
         r.K = B.wts[B.prim0[a] + i] * B.wts[B.prim0[b] + j] * std::exp(-al * be / p * ab2);
-        r.pad = 0.0;
+        r.Kp = std::sqrt(kTwoPi25) * r.K * r.inv_p;
         pp.push_back(r);
       }
   }
   // Schwarz factors on the device (scratch buffers), one launch per pair class.
-  DevBuf<PrimPair> d_pp;
-  DevBuf<int> d_pa, d_pb, d_p0, d_pn;
-  DevBuf<double> d_xyz, d_Q;
+  DevBuf<PrimPair>& d_pp = ctx->sch_pp;
+  DevBuf<int>&d_pa = ctx->sch_pa, &d_pb = ctx->sch_pb, &d_p0 = ctx->sch_p0, &d_pn = ctx->sch_pn;
+  DevBuf<double>&d_xyz = ctx->sch_xyz, &d_Q = ctx->sch_Q;
   int rc;
   if ((rc = upload(ctx, d_pp, pp)) != DSS_OK) return rc;
   if ((rc = upload(ctx, d_pa, pa)) != DSS_OK) return rc;

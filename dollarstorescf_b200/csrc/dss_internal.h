@@ -57,7 +57,15 @@ struct BasisHost {
   int nbf = 0;
   std::vector<int> l, nprim, prim0, f0;
   std::vector<double> xyz, exps, wts;
+  std::vector<double> coefs;  // the file's contraction coefficients (unnormalised)
   std::vector<int> mol;  // per shell: molecule of a batch (empty: one molecule); f0 is then molecule-local
+};
+
+// Device scratch of the one-electron kernels (grow-only, reused across calls).
+struct OneEScratch {
+  DevBuf<int2> pairs;
+  DevBuf<int> ints;
+  DevBuf<double> dbl;
 };
 
 struct ClassTasks {
@@ -94,6 +102,13 @@ struct dss_ctx {
   DevBuf<double> d_sh_xyz, d_Q, d_Qs;  // Schwarz factors: computation order, sorted pair order
   DevBuf<int> d_sh_nf;                  // functions per shell
   DevBuf<float> d_dmax;
+  // Set-up scratch, grow-only so that admitting molecule after molecule does not
+  // allocate and free device memory every time: Schwarz-factor inputs and outputs
+  // (dss_pairs_make) and the one-electron kernels' inputs.
+  DevBuf<PrimPair> sch_pp;
+  DevBuf<int> sch_pa, sch_pb, sch_p0, sch_pn;
+  DevBuf<double> sch_xyz, sch_Q;
+  OneEScratch oe_scratch;
   std::vector<int> h_pair_a, h_pair_b, h_pair_npp, h_pair_cls;
   std::vector<double> h_Q;
   std::vector<int> class_pair0, class_pair1;
@@ -112,6 +127,11 @@ struct dss_ctx {
   // build scratch
   DevBuf<double> packed_in, packed_j, packed_k, Ddense, Jacc, Kacc;
   ScfBuffers scf;
+  // Orbitals of the last dss_scf_solve / dss_uhf_solve (host copies): per spin
+  // C (n x n row-major, AO row, MO column) and the orbital energies.
+  std::vector<double> last_C[2], last_eps[2];
+  int last_nocc[2] = {0, 0};
+  int last_spins = 0;  // 0: none, 1: RHF, 2: UHF
 
   void release_basis() {
     d_pp.free();
@@ -176,10 +196,11 @@ int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* ex
 // computed on the device on stream s (synchronous).  V == NULL: T receives
 // T + V, the core Hamiltonian.
 int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz,
-                            double* S, double* T, double* V, std::string* err);
+                            double* S, double* T, double* V, std::string* err, OneEScratch* scratch = nullptr);
 // The same into host packed-U arrays (any may be NULL), plus the nuclear repulsion.
 int dss_one_electron_basis(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz,
-                           double* S, double* T, double* V, double* e_nuc, std::string* err);
+                           double* S, double* T, double* V, double* e_nuc, std::string* err,
+                           OneEScratch* scratch = nullptr);
 // sum_{A<B} Z_A Z_B / R_AB.
 double dss_nuclear_repulsion(int natom, const int* Z, const double* xyz);
 int dss_build_tasks(dss_ctx* ctx);

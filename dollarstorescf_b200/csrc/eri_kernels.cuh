@@ -192,90 +192,122 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
   const int fa = __ldg(a.sh_f0 + sa), fb = __ldg(a.sh_f0 + sb);
   const int fc = __ldg(a.sh_f0 + sc), fd = __ldg(a.sh_f0 + sd);
   const double* __restrict__ D = Dm;
+  const double s2 = 2.0 * s;
 
-  // Density blocks.
-  double dab[NA * NB], dcd[NC * ND], dad[NA * ND], dbd[NB * ND], dac[NA * NC], dbc[NB * NC];
-#pragma unroll
-  for (int i = 0; i < NA; ++i)
-#pragma unroll
-    for (int j = 0; j < NB; ++j) dab[i * NB + j] = __ldg(D + (size_t)(fa + i) * n + fb + j);
-#pragma unroll
-  for (int k = 0; k < NC; ++k)
-#pragma unroll
-    for (int l = 0; l < ND; ++l) dcd[k * ND + l] = __ldg(D + (size_t)(fc + k) * n + fd + l);
-#pragma unroll
-  for (int i = 0; i < NA; ++i) {
-#pragma unroll
-    for (int l = 0; l < ND; ++l) dad[i * ND + l] = __ldg(D + (size_t)(fa + i) * n + fd + l);
-#pragma unroll
-    for (int k = 0; k < NC; ++k) dac[i * NC + k] = __ldg(D + (size_t)(fa + i) * n + fc + k);
-  }
-#pragma unroll
-  for (int j = 0; j < NB; ++j) {
-#pragma unroll
-    for (int l = 0; l < ND; ++l) dbd[j * ND + l] = __ldg(D + (size_t)(fb + j) * n + fd + l);
-#pragma unroll
-    for (int k = 0; k < NC; ++k) dbc[j * NC + k] = __ldg(D + (size_t)(fb + j) * n + fc + k);
-  }
-
-  double jab[NA * NB], jcd[NC * ND], kad[NA * ND], kbd[NB * ND], kac[NA * NC], kbc[NB * NC];
-#pragma unroll
-  for (int q = 0; q < NA * NB; ++q) jab[q] = 0.0;
-#pragma unroll
-  for (int q = 0; q < NC * ND; ++q) jcd[q] = 0.0;
-#pragma unroll
-  for (int q = 0; q < NA * ND; ++q) kad[q] = 0.0;
-#pragma unroll
-  for (int q = 0; q < NB * ND; ++q) kbd[q] = 0.0;
-#pragma unroll
-  for (int q = 0; q < NA * NC; ++q) kac[q] = 0.0;
-#pragma unroll
-  for (int q = 0; q < NB * NC; ++q) kbc[q] = 0.0;
-
-#pragma unroll
-  for (int i = 0; i < NA; ++i)
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int k = 0; k < NC; ++k)
-#pragma unroll
-        for (int l = 0; l < ND; ++l) {
-          const double v = s * I[((i * NB + j) * NC + k) * ND + l];
-          jab[i * NB + j] += v * dcd[k * ND + l];
-          jcd[k * ND + l] += v * dab[i * NB + j];
-          kad[i * ND + l] += v * dbc[j * NC + k];
-          kbd[j * ND + l] += v * dac[i * NC + k];
-          kac[i * NC + k] += v * dbd[j * ND + l];
-          kbc[j * NC + k] += v * dad[i * ND + l];
-        }
-
-  // Bra-pair J block: same target for the whole warp.
-#pragma unroll
-  for (int i = 0; i < NA; ++i)
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-      const double v = warp_sum(jab[i * NB + j]);
-      if (lane == 0) atomicAdd(Jm + (size_t)(fa + i) * n + fb + j, 2.0 * v);
-    }
-  if (active) {
+  // One target block at a time: its density block in, its sums out, so only
+  // I, one density block and one accumulator block are live together.
+  // Bra-pair J block (Jacc[i][j] += 2 s (ij|kl) D[k][l]): the whole warp shares
+  // the target, so the lanes' sums are reduced before one atomic.
+  {
+    double d[NC * ND];
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-      for (int l = 0; l < ND; ++l) atomicAdd(Jm + (size_t)(fc + k) * n + fd + l, 2.0 * jcd[k * ND + l]);
+      for (int l = 0; l < ND; ++l) d[k * ND + l] = __ldg(D + (size_t)(fc + k) * n + fd + l);
 #pragma unroll
-    for (int i = 0; i < NA; ++i) {
+    for (int i = 0; i < NA; ++i)
 #pragma unroll
-      for (int l = 0; l < ND; ++l) atomicAdd(Km + (size_t)(fa + i) * n + fd + l, kad[i * ND + l]);
+      for (int j = 0; j < NB; ++j) {
+        double v = 0.0;
 #pragma unroll
-      for (int k = 0; k < NC; ++k) atomicAdd(Km + (size_t)(fa + i) * n + fc + k, kac[i * NC + k]);
-    }
+        for (int q = 0; q < NC * ND; ++q) v += I[(i * NB + j) * NC * ND + q] * d[q];
+        v = warp_sum(s2 * v);
+        if (lane == 0) atomicAdd(Jm + (size_t)(fa + i) * n + fb + j, v);
+      }
+  }
+  if (!active) return;
+  // Jacc[k][l] += 2 s (ij|kl) D[i][j]
+  {
+    double d[NA * NB];
 #pragma unroll
-    for (int j = 0; j < NB; ++j) {
+    for (int i = 0; i < NA; ++i)
 #pragma unroll
-      for (int l = 0; l < ND; ++l) atomicAdd(Km + (size_t)(fb + j) * n + fd + l, kbd[j * ND + l]);
+      for (int j = 0; j < NB; ++j) d[i * NB + j] = __ldg(D + (size_t)(fa + i) * n + fb + j);
 #pragma unroll
-      for (int k = 0; k < NC; ++k) atomicAdd(Km + (size_t)(fb + j) * n + fc + k, kbc[j * NC + k]);
-    }
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) {
+        double v = 0.0;
+#pragma unroll
+        for (int q = 0; q < NA * NB; ++q) v += I[q * NC * ND + k * ND + l] * d[q];
+        atomicAdd(Jm + (size_t)(fc + k) * n + fd + l, s2 * v);
+      }
+  }
+  // Kacc[i][l] += s (ij|kl) D[j][k]
+  {
+    double d[NB * NC];
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) d[j * NC + k] = __ldg(D + (size_t)(fb + j) * n + fc + k);
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) {
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) v += I[((i * NB + j) * NC + k) * ND + l] * d[j * NC + k];
+        atomicAdd(Km + (size_t)(fa + i) * n + fd + l, s * v);
+      }
+  }
+  // Kacc[j][l] += s (ij|kl) D[i][k]
+  {
+    double d[NA * NC];
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) d[i * NC + k] = __ldg(D + (size_t)(fa + i) * n + fc + k);
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) {
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) v += I[((i * NB + j) * NC + k) * ND + l] * d[i * NC + k];
+        atomicAdd(Km + (size_t)(fb + j) * n + fd + l, s * v);
+      }
+  }
+  // Kacc[i][k] += s (ij|kl) D[j][l]
+  {
+    double d[NB * ND];
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) d[j * ND + l] = __ldg(D + (size_t)(fb + j) * n + fd + l);
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+          for (int l = 0; l < ND; ++l) v += I[((i * NB + j) * NC + k) * ND + l] * d[j * ND + l];
+        atomicAdd(Km + (size_t)(fa + i) * n + fc + k, s * v);
+      }
+  }
+  // Kacc[j][k] += s (ij|kl) D[i][l]
+  {
+    double d[NA * ND];
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) d[i * ND + l] = __ldg(D + (size_t)(fa + i) * n + fd + l);
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+          for (int l = 0; l < ND; ++l) v += I[((i * NB + j) * NC + k) * ND + l] * d[i * ND + l];
+        atomicAdd(Km + (size_t)(fb + j) * n + fc + k, s * v);
+      }
   }
 }
 

@@ -311,7 +311,7 @@ void launch_one_e_class(int la, int lb, const OneEArgs& a, cudaStream_t s) {
 }  // namespace
 
 int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz_bohr,
-                            double* dS, double* dT, double* dV, std::string* errp) {
+                            double* dS, double* dT, double* dV, std::string* errp, OneEScratch* scratch) {
   const int ns = (int)B.l.size();
   for (int q = 0; q < ns; ++q)
     if (B.l[q] < 0 || B.l[q] > kLmaxOne) {
@@ -357,9 +357,11 @@ int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const
   hd.insert(hd.end(), xyz_bohr, xyz_bohr + 3 * (size_t)natom);
   hd.insert(hd.end(), zd.begin(), zd.end());
   hd.insert(hd.end(), tr.begin(), tr.end());
-  DevBuf<int2> d_pairs;
-  DevBuf<int> d_i;
-  DevBuf<double> d_d;
+  OneEScratch local;
+  OneEScratch& sc = scratch ? *scratch : local;
+  DevBuf<int2>& d_pairs = sc.pairs;
+  DevBuf<int>& d_i = sc.ints;
+  DevBuf<double>& d_d = sc.dbl;
   cudaError_t e = d_pairs.resize(std::max<size_t>(pairs.size(), 1));
   if (e == cudaSuccess) e = d_i.resize(std::max<size_t>(ni, 1));
   if (e == cudaSuccess) e = d_d.resize(std::max<size_t>(hd.size(), 1));
@@ -400,7 +402,7 @@ int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const
     launch_one_e_class(c / 3, c % 3, a, s);
   }
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the input buffers are freed on return
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the inputs are freed or reused after return
   if (e != cudaSuccess) {
     if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
     return DSS_ERR_CUDA;
@@ -421,7 +423,8 @@ double dss_nuclear_repulsion(int natom, const int* Z, const double* xyz_bohr) {
 }
 
 int dss_one_electron_basis(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz_bohr,
-                           double* S_packed, double* T_packed, double* V_packed, double* e_nuc, std::string* errp) {
+                           double* S_packed, double* T_packed, double* V_packed, double* e_nuc, std::string* errp,
+                           OneEScratch* scratch) {
   const size_t np = (size_t)B.nbf * (B.nbf + 1) / 2;
   DevBuf<double> d;
   cudaError_t e = d.resize(std::max<size_t>(3 * np, 1));
@@ -429,7 +432,7 @@ int dss_one_electron_basis(cudaStream_t s, const BasisHost& B, int natom, const 
     if (errp) *errp = std::string("dss_one_electron: ") + cudaGetErrorString(e);
     return DSS_ERR_OOM;
   }
-  int rc = dss_one_electron_device(s, B, natom, Z, xyz_bohr, d.ptr, d.ptr + np, d.ptr + 2 * np, errp);
+  int rc = dss_one_electron_device(s, B, natom, Z, xyz_bohr, d.ptr, d.ptr + np, d.ptr + 2 * np, errp, scratch);
   if (rc != DSS_OK) return rc;
   double* outs[3] = {S_packed, T_packed, V_packed};
   for (int k = 0; k < 3 && e == cudaSuccess; ++k)
@@ -453,7 +456,7 @@ extern "C" int dss_one_electron(dss_ctx* ctx, int natom, const int* Z, const dou
   cudaSetDevice(ctx->opts.device);
   std::string err;
   const int rc = dss_one_electron_basis(ctx->stream, ctx->basis, natom, Z, xyz_bohr, S_packed, T_packed, V_packed,
-                                        e_nuc, &err);
+                                        e_nuc, &err, &ctx->oe_scratch);
   if (rc != DSS_OK) return dss_fail(ctx, rc, err);
   return DSS_OK;
 }

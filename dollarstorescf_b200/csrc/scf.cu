@@ -444,7 +444,15 @@ int dss_scf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
     pack_sym<<<nb(n2), 256, 0, s>>>(D, packed.ptr, n);
     SCF_CHECK(cudaMemcpyAsync(Dp, packed.ptr, np * 8, cudaMemcpyDeviceToHost, s), "D2H D");
   }
+  // The final orbitals, for dss_scf_orbitals / dss_write_molden.
+  ctx->last_C[0].resize(n2);
+  ctx->last_eps[0].resize(n);
+  SCF_CHECK(cudaMemcpyAsync(ctx->last_C[0].data(), C, n2 * 8, cudaMemcpyDeviceToHost, s), "D2H C");
+  SCF_CHECK(cudaMemcpyAsync(ctx->last_eps[0].data(), eps, (size_t)n * 8, cudaMemcpyDeviceToHost, s), "D2H eps");
   SCF_CHECK(cudaStreamSynchronize(s), "sync");
+  ctx->last_nocc[0] = n_alpha;
+  ctx->last_nocc[1] = 0;
+  ctx->last_spins = 1;
   *E_total = 2.0 * tr[0] + tr[1] + e_nuc;
   if (iterations) *iterations = it;
 #undef SCF_CHECK
@@ -618,6 +626,18 @@ int dss_uhf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
     UHF_CHECK(cudaMemcpyAsync(out, packed.ptr, np * 8, cudaMemcpyDeviceToHost, s), "D2H D");
     UHF_CHECK(cudaStreamSynchronize(s), "sync");
   }
+  for (int sp = 0; sp < 2; ++sp) {  // the final orbitals, for dss_scf_orbitals / dss_write_molden
+    dss_gemm(s, n, false, false, 1.0, X, Cp[sp], 0.0, C);
+    ctx->last_C[sp].resize(n2);
+    ctx->last_eps[sp].resize(n);
+    UHF_CHECK(cudaMemcpyAsync(ctx->last_C[sp].data(), C, n2 * 8, cudaMemcpyDeviceToHost, s), "D2H C");
+    UHF_CHECK(cudaMemcpyAsync(ctx->last_eps[sp].data(), eps[sp], (size_t)n * 8, cudaMemcpyDeviceToHost, s),
+              "D2H eps");
+    UHF_CHECK(cudaStreamSynchronize(s), "sync");
+  }
+  ctx->last_nocc[0] = n_alpha;
+  ctx->last_nocc[1] = n_beta;
+  ctx->last_spins = 2;
   UHF_CHECK(cudaStreamSynchronize(s), "sync");
   // tr(Ds Gs) = tr(Ds J) - tr(Ds Ks); summed over the spins: tr(Dt J) - sum tr(Ds Ks).
   const double exch = tr[1] - (tr[2] + tr[3]);  // sum_s tr(Ds Ks)

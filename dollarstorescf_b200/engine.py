@@ -209,6 +209,21 @@ class FockBuilder:
             self._check(rc)
         return E.value, Da, Db, it.value, rc
 
+    def orbitals(self, spin: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        """(C [AO, MO], orbital energies) of the last scf()/uhf() for one spin."""
+        n = self.nbf
+        C = np.empty((n, n))
+        eps = np.empty(n)
+        self._check(self._L.dss_scf_orbitals(self._h, int(spin), _dp(C), _dp(eps)))
+        return C, eps
+
+    def write_molden(self, path: str, sh: ShellArrays, write_virtual: bool = True) -> None:
+        """Molden file of the last scf()/uhf() (scf::writeOrbitalsMolden)."""
+        Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
+        xyz = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
+        self._check(self._L.dss_write_molden(self._h, path.encode(), sh.natom, _ip(Z), _dp(xyz),
+                                             1 if write_virtual else 0))
+
     def sync(self) -> None:
         self._check(self._L.dss_sync(self._h))
 

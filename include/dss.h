@@ -215,6 +215,20 @@ int dss_uhf_solve(dss_ctx* ctx, const double* H_packed, const double* S_packed, 
                   double e_nuc, const dss_scf_opts* opts, double* E_total, double* D_alpha_inout,
                   double* D_beta_inout, int* iterations);
 
+/* MO coefficients (n x n row-major: AO row, MO column, ascending orbital
+ * energy) and orbital energies of spin 0 (alpha; the RHF orbitals) or 1 (beta,
+ * after dss_uhf_solve) from the last solve in this context: the reference's
+ * scf::coefficient_matrix[spin] and scf::mo_levels[spin]
+ * (chem/scf/SCFCommon.hpp:28-29).  Either output may be NULL. */
+int dss_scf_orbitals(const dss_ctx* ctx, int spin, double* C, double* eps);
+
+/* Molden file of the last solve, replacing scf::writeOrbitalsMolden
+ * (chem/scf/WriteOrbitals.cpp:17-137): nuclei Z[natom] / xyz_bohr (the shells'
+ * centres), the basis with its file coefficients, the orbitals (all of them when
+ * write_virtual, else the occupied ones), alpha then beta.  5D bases only. */
+int dss_write_molden(dss_ctx* ctx, const char* path, int natom, const int* Z, const double* xyz_bohr,
+                     int write_virtual);
+
 /* ---------------------------------------------------------------- batches of molecules */
 /* Many closed-shell molecules of uneven size solved together: each ERI class
  * is one launch over every molecule of the batch, and one SCF iteration of all

@@ -31,6 +31,7 @@
 #include "chem/scf/SCFBasis.hpp"
 #include "chem/scf/SCFCommon.hpp"
 #include "chem/scf/SCFSolver.hpp"
+#include "chem/scf/WriteOrbitals.hpp"
 
 namespace flo {
 double boysFunctionExact(double x, uint m);
@@ -226,6 +227,13 @@ int ref_scf(double conv, double* E_total, double* D_alpha_packed, double* second
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   if (quiet) quiet_off();
   return (int)scf::iteration;
+}
+
+// Molden file of the last ref_scf (scf::writeOrbitalsMolden, chem/scf/WriteOrbitals.cpp:17-137).
+void ref_write_molden(const char* path, int write_virtual, int quiet) {
+  if (quiet) quiet_on();
+  scf::writeOrbitalsMolden(std::string(path), write_virtual != 0);
+  if (quiet) quiet_off();
 }
 
 // Spin density (0 = alpha, 1 = beta; packed-U) after ref_scf, and the

@@ -42,6 +42,7 @@ def lib():
         L.ref_scf.argtypes = [ctypes.c_double, dp, dp, dp, ctypes.c_int]
         L.ref_scf.restype = ctypes.c_int
         L.ref_get_density.argtypes = [ctypes.c_int, dp]
+        L.ref_write_molden.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
         L.ref_electron_counts.argtypes = [ip, ip]
         L.ref_fock_2e.argtypes = [dp, dp]
         L.ref_fock_2e.restype = ctypes.c_int
@@ -99,6 +100,11 @@ def spin_density(spin: int) -> np.ndarray:
     D = np.zeros(n * (n + 1) // 2)
     L.ref_get_density(int(spin), _p(D))
     return D
+
+
+def write_molden(path: str, write_virtual: bool = True) -> None:
+    """The reference's Molden file of the last scf() call."""
+    lib().ref_write_molden(path.encode(), 1 if write_virtual else 0, 1)
 
 
 def electron_counts() -> Tuple[int, int]:

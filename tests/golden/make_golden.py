@@ -7,6 +7,9 @@ oracle/build_ref.sh and driven through oracle/ref_harness.cpp:
                    energy (|dE| < 1e-10), the final alpha density (packed-U),
                    J[D_total], K[D_alpha] and G = J - K at that density, the
                    same three for a seeded random symmetric density, S and H.
+  * <name>.molden  the reference's Molden files (scf::writeOrbitalsMolden, virtual
+                   orbitals included) of water 6-31G* (RHF) and CH2 triplet
+                   6-31G* (UHF) after converged solves
   * <name>_uhf.npz open-shell molecules (multiplicity > 1, the reference's
                    unrestricted branch): charge, multiplicity, electron counts,
                    the converged energy and both final spin densities, S and H.
@@ -84,8 +87,26 @@ def write_uhf_case(name, mol, bas, pure, charge, mult) -> None:
     print(f"{name:18s} n={n:4d} na={na} nb={nb} E={E:.13f} it={it} ({secs:.2f}s)")
 
 
+def write_molden_cases() -> None:
+    A = basis.molecule_from_angstrom
+    for name, mol, bas, charge, mult in (
+            ("water_631gs", geometry.water(), "6-31G*", 0, 1),
+            ("ch2_631gs_uhf", A(["C", "H", "H"], [[0, 0, 0], [0.9918, 0.4226, 0], [-0.9918, 0.4226, 0]]),
+             "6-31G*", 0, 3)):
+        sh = shells.build_shells(mol, basis.builtin_basis(bas), pure=True)
+        refpy.setup(sh, charge=charge, multiplicity=mult)
+        refpy.scf(1e-10)
+        refpy.write_molden(os.path.join(HERE, name + ".molden"), True)
+        print(f"{name}.molden")
+
+
 def main() -> None:
     only = set(sys.argv[1:])
+    if "molden" in only:
+        write_molden_cases()
+        only.discard("molden")
+        if not only:
+            return
     if only:
         rng = np.random.default_rng(1234)
         for name, mol, bas, pure in cases():
@@ -104,6 +125,7 @@ def main() -> None:
         write_case(name, mol, bas, pure, rng)
     for name, mol, bas, pure, charge, mult in uhf_cases():
         write_uhf_case(name, mol, bas, pure, charge, mult)
+    write_molden_cases()
 
 
 def write_case(name, mol, bas, pure, rng) -> None:
