@@ -92,13 +92,15 @@ def measure_rows(device: int, cpu_baseline: bool):
         fb.set_basis(sh32)
         fb.one_electron(sh32)
         ts = []
-        for _ in range(5):
+        for _ in range(11):
             t0 = _t.perf_counter()
             fb.one_electron(sh32)
             ts.append(_t.perf_counter() - t0)
     ts.sort()
-    oe = {"workload": "(H2O)32 6-31G* 6D S, T, V (608 functions, 96 nuclei)", "gpu_ms": ts[2] * 1e3,
-          "per_s": 1.0 / ts[2]}
+    # Host-side jitter (pageable copies of 3 x 1.5 MB) spreads single calls; the
+    # median of 11 is the reported figure, the fastest call beside it.
+    oe = {"workload": "(H2O)32 6-31G* 6D S, T, V (608 functions, 96 nuclei)", "gpu_ms": ts[5] * 1e3,
+          "gpu_ms_min": ts[0] * 1e3, "per_s": 1.0 / ts[5]}
     if cpu_baseline:
         from oracle import refpy
 
@@ -108,7 +110,7 @@ def measure_rows(device: int, cpu_baseline: bool):
             dt = _t.perf_counter() - t0
             oe["cpu_baseline"] = {"seconds": dt, "per_s": 1.0 / dt, "cores": 1, "kind": "reference",
                                   "sample": "the reference's basis set-up without the ERI tensor (S, T, V, X)"}
-            oe["gpu_over_cpu"] = dt / ts[2]
+            oe["gpu_over_cpu"] = dt / ts[5]
     out["one_electron"] = oe
 
     A = B.molecule_from_angstrom
