@@ -126,7 +126,7 @@ __device__ __forceinline__ double quartet_dbound(const EriArgs& a, int sa, int s
 
 // Resident blocks the compiler must allow (caps registers): the light classes
 // are latency bound and want more warps; the heavy ones keep their registers.
-__host__ __device__ constexpr int dss_min_blocks(int L) { return L == 0 ? 8 : (L <= 2 ? 7 : (L <= 4 ? 4 : 1)); }
+__host__ __device__ constexpr int dss_min_blocks(int L) { return L == 0 ? 8 : (L <= 2 ? 6 : (L <= 4 ? 4 : 1)); }
 
 template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false>
 __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk_kernel(EriArgs a) {
