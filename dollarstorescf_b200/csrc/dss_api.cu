@@ -439,18 +439,22 @@ int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out) {
   P.cls.resize(np);
   P.mol.resize(np);
   P.Q.resize(np);
+  // Primitive pairs in the final pair order, so that the kets of one warp task
+  // (consecutive pairs of equal primitive count) read one contiguous span.
+  P.pp.resize(pp.size() * 10);
+  size_t off = 0;
   for (int q = 0; q < np; ++q) {
     const int o = perm[q];
     P.pa[q] = pa[o];
     P.pb[q] = pb[o];
-    P.p0[q] = p0[o];
+    P.p0[q] = (int)off;
     P.pn[q] = pn[o];
     P.cls[q] = pairs[o].cls;
     P.mol[q] = pairs[o].mol;
     P.Q[q] = Q[o];
+    if (pn[o]) std::memcpy(P.pp.data() + off * 10, &pp[p0[o]], (size_t)pn[o] * sizeof(PrimPair));
+    off += pn[o];
   }
-  P.pp.resize(pp.size() * 10);
-  if (!pp.empty()) std::memcpy(P.pp.data(), pp.data(), pp.size() * sizeof(PrimPair));
   return DSS_OK;
 }
 
