@@ -53,21 +53,28 @@ def _write_if_changed(path: str, text: str) -> None:
 
 def _class_tu(c, coop: bool) -> str:
     """One translation unit per class: its kernels and host launchers.
-    Variants: Boys mode (0 reference, 1 accurate) x 5D/6D, plus the
-    mixed-precision screened form with the accurate Boys function."""
+    Variants: Boys mode (0 reference, 1 accurate) x 5D/6D, the mixed-precision
+    screened form with the accurate Boys function, and the unrestricted
+    (two-density) form with the reference Boys function."""
     la, lb, lc, ld = c
     name = f"{la}{lb}{lc}{ld}"
     lines = [f'#include "{"coop_kernels.cuh" if coop else "eri_kernels.cuh"}"', ""]
     combos = [(0, 1, 0), (0, 0, 0), (1, 1, 0), (1, 0, 0), (1, 1, 1), (1, 0, 1)]
-    lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, const EriArgs& a, cudaStream_t s) {{")
+    lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, int uhf, const EriArgs& a, "
+                 f"cudaStream_t s) {{")
     lines.append("  const int threads = 128;")
     lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
     lines.append("  if (!blocks) return;")
     for boys, pure, mixed in combos:
         pb = "true" if pure else "false"
         mb = "true" if mixed else "false"
-        lines.append(f"  if (boys == {boys} && pure == {pure} && mixed == {mixed}) "
+        lines.append(f"  if (!uhf && boys == {boys} && pure == {pure} && mixed == {mixed}) "
                      f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}><<<blocks, threads, 0, s>>>(a);")
+    # The unrestricted variant: FP64 with the reference-mode Boys function.
+    for pure in (1, 0):
+        pb = "true" if pure else "false"
+        lines.append(f"  if (uhf && pure == {pure}) "
+                     f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, true><<<blocks, threads, 0, s>>>(a);")
     lines.append("}")
     if (la, lb) == (lc, ld):
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s) {{")
@@ -112,12 +119,12 @@ def _dispatch_tu(classes, pcls, coop) -> str:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) return true;")
     lines.append("  return false;")
     lines.append("}")
-    lines.append("void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int variant, "
-                 "const EriArgs& a, cudaStream_t s) {")
+    lines.append("void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, "
+                 "int variant, const EriArgs& a, cudaStream_t s) {")
     for (la, lb, lc, ld) in coop:
-        lines.append(f"  if (variant == 1 && la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
+        lines.append(f"  if (!uhf && variant == 1 && la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
                      f"return dss_launch_eri_coop_{la}{lb}{lc}{ld}(boys, pure, mixed, a, s);")
-    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, mixed, a, s);")
+    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, mixed, uhf, a, s);")
     lines.append("}")
     for (la, lb) in pcls:
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s);")
@@ -125,11 +132,11 @@ def _dispatch_tu(classes, pcls, coop) -> str:
     for (la, lb) in pcls:
         lines.append(f"  if (la == {la} && lb == {lb}) return dss_launch_schwarz_{la}{lb}(boys, pure, a, s);")
     lines.append("}")
-    lines.append("void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, "
+    lines.append("void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, "
                  "const EriArgs& a, cudaStream_t s) {")
     for (la, lb, lc, ld) in classes:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
-                     f"return dss_launch_eri_jk_{la}{lb}{lc}{ld}(boys, pure, mixed, a, s);")
+                     f"return dss_launch_eri_jk_{la}{lb}{lc}{ld}(boys, pure, mixed, uhf, a, s);")
     lines.append("}")
     return "\n".join(lines) + "\n"
 

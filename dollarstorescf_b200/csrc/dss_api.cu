@@ -647,9 +647,12 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   const bool batch = ctx->nmol > 0;
   const int n = ctx->nbf;
   const size_t nn = (size_t)n * n;
+  if (mode->uhf && (batch || mode->mixed || mode->boys != DSS_BOYS_REF || !mode->Da || !mode->Db || !mode->K2))
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_enqueue_jk: the unrestricted build is FP64, reference Boys, one molecule");
   if (!mode->no_zero) {
     DSS_CUDA(cudaMemsetAsync(Jacc, 0, nn * sizeof(double), ctx->stream));
     DSS_CUDA(cudaMemsetAsync(Kacc, 0, nn * sizeof(double), ctx->stream));
+    if (mode->uhf) DSS_CUDA(cudaMemsetAsync(mode->K2, 0, nn * sizeof(double), ctx->stream));
   }
   // Launch order: highest total angular momentum first (longest per-quartet
   // latency), spread round-robin over the side streams; profiling (events)
@@ -702,9 +705,12 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.skip_thr = mode->skip_thr;
     a.fp32_thr = mode->fp32_thr;
     a.boys_cell = ctx->boys_cell;
+    a.Da = mode->Da;
+    a.Db = mode->Db;
+    a.K2 = mode->K2;
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], st));
     dss_launch_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, mode->mixed ? DSS_BOYS_FAST : mode->boys, ctx->pure,
-                           mode->mixed, ct.variant, a, st);
+                           mode->mixed, mode->uhf ? 1 : 0, ct.variant, a, st);
     DSS_CUDA(cudaGetLastError());
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], st));
   }

@@ -214,6 +214,12 @@ struct BuildMode {
   const float* dmax = nullptr;
   double skip_thr = 0.0, fp32_thr = 0.0;
   bool no_zero = false;  // the caller has zeroed the accumulators (batch mode)
+  // Unrestricted build (one molecule): J from D = D_a + D_b, K from Da into
+  // Kacc and from Db into K2 (zeroed here unless no_zero).
+  bool uhf = false;
+  const double* Da = nullptr;
+  const double* Db = nullptr;
+  double* K2 = nullptr;
 };
 
 // Enqueues one J/K accumulation; with events != NULL records events[2i], events[2i+1]

@@ -58,6 +58,11 @@ struct EriArgs {
   const int* sh_nsm;
   const int* mol_active;
   const double* boys_cell;  // reference-mode Boys records (dss_boys_cell_table)
+  // Unrestricted builds (the UHF kernel variant, one molecule): J from D (the
+  // total density D_a + D_b), K from Da into K and from Db into K2.
+  const double* Da;
+  const double* Db;
+  double* K2;
 };
 
 struct SchwarzArgs {
@@ -128,7 +133,92 @@ __device__ __forceinline__ double quartet_dbound(const EriArgs& a, int sa, int s
 // are latency bound and want more warps; the heavy ones keep their registers.
 __host__ __device__ constexpr int dss_min_blocks(int L) { return L == 0 ? 8 : (L <= 2 ? 6 : (L <= 4 ? 4 : 1)); }
 
-template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false>
+// The four exchange target blocks of one quartet (Kacc[i][l] += s (ij|kl) D[j][k]
+// and the three others), one block at a time, from density D into Km.
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void digest_k(const double* I, double s, const double* __restrict__ D, double* Km, int n,
+                                         int fa, int fb, int fc, int fd) {
+  // Kacc[i][l] += s (ij|kl) D[j][k]
+  {
+    double d[NB * NC];
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) d[j * NC + k] = __ldg(D + (size_t)(fb + j) * n + fc + k);
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) {
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) v += I[((i * NB + j) * NC + k) * ND + l] * d[j * NC + k];
+        atomicAdd(Km + (size_t)(fa + i) * n + fd + l, s * v);
+      }
+  }
+  // Kacc[j][l] += s (ij|kl) D[i][k]
+  {
+    double d[NA * NC];
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) d[i * NC + k] = __ldg(D + (size_t)(fa + i) * n + fc + k);
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) {
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) v += I[((i * NB + j) * NC + k) * ND + l] * d[i * NC + k];
+        atomicAdd(Km + (size_t)(fb + j) * n + fd + l, s * v);
+      }
+  }
+  // Kacc[i][k] += s (ij|kl) D[j][l]
+  {
+    double d[NB * ND];
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) d[j * ND + l] = __ldg(D + (size_t)(fb + j) * n + fd + l);
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+          for (int l = 0; l < ND; ++l) v += I[((i * NB + j) * NC + k) * ND + l] * d[j * ND + l];
+        atomicAdd(Km + (size_t)(fa + i) * n + fc + k, s * v);
+      }
+  }
+  // Kacc[j][k] += s (ij|kl) D[i][l]
+  {
+    double d[NA * ND];
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+      for (int l = 0; l < ND; ++l) d[i * ND + l] = __ldg(D + (size_t)(fa + i) * n + fd + l);
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+          for (int l = 0; l < ND; ++l) v += I[((i * NB + j) * NC + k) * ND + l] * d[i * ND + l];
+        atomicAdd(Km + (size_t)(fb + j) * n + fc + k, s * v);
+      }
+  }
+}
+
+// UHF = true: the unrestricted variant (one molecule): J from a.D = D_a + D_b,
+// K from a.Da into a.K and from a.Db into a.K2, from one evaluation of the integrals.
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false, bool UHF = false>
 __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk_kernel(EriArgs a) {
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
   constexpr int NC = dss_nfunc(LC, PURE), ND = dss_nfunc(LD, PURE);
@@ -233,81 +323,11 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
         atomicAdd(Jm + (size_t)(fc + k) * n + fd + l, s2 * v);
       }
   }
-  // Kacc[i][l] += s (ij|kl) D[j][k]
-  {
-    double d[NB * NC];
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int k = 0; k < NC; ++k) d[j * NC + k] = __ldg(D + (size_t)(fb + j) * n + fc + k);
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) {
-        double v = 0.0;
-#pragma unroll
-        for (int j = 0; j < NB; ++j)
-#pragma unroll
-          for (int k = 0; k < NC; ++k) v += I[((i * NB + j) * NC + k) * ND + l] * d[j * NC + k];
-        atomicAdd(Km + (size_t)(fa + i) * n + fd + l, s * v);
-      }
-  }
-  // Kacc[j][l] += s (ij|kl) D[i][k]
-  {
-    double d[NA * NC];
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-#pragma unroll
-      for (int k = 0; k < NC; ++k) d[i * NC + k] = __ldg(D + (size_t)(fa + i) * n + fc + k);
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) {
-        double v = 0.0;
-#pragma unroll
-        for (int i = 0; i < NA; ++i)
-#pragma unroll
-          for (int k = 0; k < NC; ++k) v += I[((i * NB + j) * NC + k) * ND + l] * d[i * NC + k];
-        atomicAdd(Km + (size_t)(fb + j) * n + fd + l, s * v);
-      }
-  }
-  // Kacc[i][k] += s (ij|kl) D[j][l]
-  {
-    double d[NB * ND];
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) d[j * ND + l] = __ldg(D + (size_t)(fb + j) * n + fd + l);
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-#pragma unroll
-      for (int k = 0; k < NC; ++k) {
-        double v = 0.0;
-#pragma unroll
-        for (int j = 0; j < NB; ++j)
-#pragma unroll
-          for (int l = 0; l < ND; ++l) v += I[((i * NB + j) * NC + k) * ND + l] * d[j * ND + l];
-        atomicAdd(Km + (size_t)(fa + i) * n + fc + k, s * v);
-      }
-  }
-  // Kacc[j][k] += s (ij|kl) D[i][l]
-  {
-    double d[NA * ND];
-#pragma unroll
-    for (int i = 0; i < NA; ++i)
-#pragma unroll
-      for (int l = 0; l < ND; ++l) d[i * ND + l] = __ldg(D + (size_t)(fa + i) * n + fd + l);
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-#pragma unroll
-      for (int k = 0; k < NC; ++k) {
-        double v = 0.0;
-#pragma unroll
-        for (int i = 0; i < NA; ++i)
-#pragma unroll
-          for (int l = 0; l < ND; ++l) v += I[((i * NB + j) * NC + k) * ND + l] * d[i * ND + l];
-        atomicAdd(Km + (size_t)(fb + j) * n + fc + k, s * v);
-      }
+  if constexpr (UHF) {
+    digest_k<NA, NB, NC, ND>(I, s, a.Da, Km, n, fa, fb, fc, fd);
+    digest_k<NA, NB, NC, ND>(I, s, a.Db, a.K2, n, fa, fb, fc, fd);
+  } else {
+    digest_k<NA, NB, NC, ND>(I, s, D, Km, n, fa, fb, fc, fd);
   }
 }
 
@@ -337,14 +357,15 @@ __global__ void __launch_bounds__(128) schwarz_kernel(SchwarzArgs a) {
 
 // Host-side launchers (one translation unit per class defines them).
 #define DSS_DECLARE_LAUNCHERS(la, lb, lc, ld, bc, kc) \
-  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, int mixed, const EriArgs& a, cudaStream_t s);
+  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, int mixed, int uhf, const EriArgs& a, cudaStream_t s);
 DSS_FOR_EACH_CLASS(DSS_DECLARE_LAUNCHERS)
 #undef DSS_DECLARE_LAUNCHERS
 
 void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s);
 // variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class).
-void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int variant,
+// uhf = 1: the unrestricted variant (thread per quartet, reference Boys only).
+void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, int variant,
                             const EriArgs& a, cudaStream_t s);
 bool dss_has_coop(int la, int lb, int lc, int ld);
-void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, const EriArgs& a,
+void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, const EriArgs& a,
                        cudaStream_t s);

@@ -238,6 +238,21 @@ __global__ void uhf_combine(const double* __restrict__ Ja, const double* __restr
   if (Jt) Jt[t] = J;
 }
 
+// The same from one unrestricted build: J accumulated from D_a + D_b, one
+// exchange accumulator per spin.
+__global__ void uhf_combine_one(const double* __restrict__ Jacc, const double* __restrict__ Ka,
+                                const double* __restrict__ Kb, double* __restrict__ Ga, double* __restrict__ Gb,
+                                double* __restrict__ Jt, int n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int r = (int)(t / n), c = (int)(t % n);
+  const long long u = (long long)c * n + r;
+  const double J = Jacc[t] + Jacc[u];
+  Ga[t] = J - (Ka[t] + Ka[u]);
+  Gb[t] = J - (Kb[t] + Kb[u]);
+  if (Jt) Jt[t] = J;
+}
+
 // E_elec = sum_{i<na} eps_a_i + sum_{i<nb} eps_b_i - (tr(Da Ga) + tr(Db Gb)) / 2
 // (getTotalElectronicEnergy, unrestricted branch, SCFSolver.cpp:131-142).
 __global__ void uhf_energy_kernel(const double* eps_a, int na, const double* eps_b, int nbeta, const double* tr,
@@ -535,8 +550,22 @@ int dss_uhf_solve(dss_ctx* ctx, const double* Hp, const double* Sp, int n_alpha,
   UHF_CHECK(cudaMemsetAsync(b.ibuf.ptr, 0, 16 * sizeof(int), s), "zero state");
   BuildMode mode;
   mode.boys = ctx->opts.boys_mode;
-  // J and K of both spin densities, combined into G_a, G_b (and J).
+  // J of the total density and K of each spin density, combined into G_a, G_b
+  // (and J).  With the reference Boys function one unrestricted build evaluates
+  // every integral once for both exchange matrices; otherwise one build per spin.
   auto two_electron = [&]() -> int {
+    if (mode.boys == DSS_BOYS_REF) {
+      axpby<<<nb(n2), 256, 0, s>>>((long long)n2, 1.0, D[0], 1.0, D[1], 0.0, nullptr, T1);  // D_a + D_b
+      BuildMode um = mode;
+      um.uhf = true;
+      um.Da = D[0];
+      um.Db = D[1];
+      um.K2 = Kacc[1];
+      int r = dss_enqueue_jk(ctx, T1, Jacc[0], Kacc[0], nullptr, &um);
+      if (r != DSS_OK) return r;
+      uhf_combine_one<<<nb(n2), 256, 0, s>>>(Jacc[0], Kacc[0], Kacc[1], G[0], G[1], Jt, n);
+      return DSS_OK;
+    }
     for (int sp = 0; sp < 2; ++sp) {
       int r = dss_enqueue_jk(ctx, D[sp], Jacc[sp], Kacc[sp], nullptr, &mode);
       if (r != DSS_OK) return r;

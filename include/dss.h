@@ -205,7 +205,9 @@ int dss_scf_solve(dss_ctx* ctx, const double* H_packed, const double* S_packed, 
  * scf::assignMolecule, chem/scf/SCFBasis.cpp:17-37), replacing the
  * unrestricted branch of scf::solveMOs + scf::calculateEnergies
  * (chem/scf/SCFSolver.cpp:120-172,196-237; chem/scf/Energy.cpp:21-50):
- * G_s = J[D_a + D_b] - K[D_s] from two J/K builds per iteration, one Pulay DIIS
+ * G_s = J[D_a + D_b] - K[D_s] from one unrestricted J/K build per iteration (each
+ * integral evaluated once for J and both exchange matrices; two builds with the
+ * accurate Boys mode), one Pulay DIIS
  * ring per spin (chem/scf/SCFDIIS.cpp:14-52), one eigensolve per spin,
  * E_elec = sum eps_a + sum eps_b - (tr(D_a G_a) + tr(D_b G_b))/2.  n_alpha and
  * n_beta occupied orbitals (electron_count[0], electron_count[1]).  Plain FP64
