@@ -217,6 +217,24 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- replicas
+def max_over_ranks(x: float, device: str) -> float:
+    """The largest of every rank's x (an all-reduce MAX on the process group):
+    the job's time is the slowest replica's."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world_size: int, steps: int, seconds: float) -> float:
+    """Whole-job builds/s of world_size independent replicas that each ran
+    `steps` builds, timed by the slowest one (weak scaling)."""
+    return world_size * steps / seconds
+
+
 # ---------------------------------------------------------------- GPU arm
 class ClockSampler:
     def __init__(self, device: int):
@@ -363,10 +381,8 @@ def run_gpu(args):
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     tot_ms = sum(step_ms)
     if ws > 1:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = ws * args.steps / (tot_ms * 1e-3)
+        tot_ms = max_over_ranks(tot_ms, f"cuda:{device}")
+    value = replica_rate(ws, args.steps, tot_ms * 1e-3)
 
     # --- e2e through the reference-facing C ABI, pinned host buffers.
     npk = n * (n + 1) // 2
@@ -386,10 +402,33 @@ def run_gpu(args):
         e2e_s.append(time.perf_counter() - t1)
     e2e_tot = sum(e2e_s)
     if ws > 1:
-        t = torch.tensor([e2e_tot], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_tot = float(t.item())
-    e2e_value = ws * args.steps / e2e_tot
+        e2e_tot = max_over_ranks(e2e_tot, f"cuda:{device}")
+    e2e_value = replica_rate(ws, args.steps, e2e_tot)
+
+    # --- mixed-precision incremental builds (G of a density change dD: FP32
+    # quartets below Schwarz.|dD| 1e-7, skipped below 1e-12), same timing rules.
+    mixed_builds = {}
+    for scale in (1e-3, 1e-5):
+        dD = torch.tensor(Dm * scale, dtype=torch.float64, device=f"cuda:{device}")
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                flush.fill_(1.0)
+                fb.jk_mixed_device(dD.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
+            stream.synchronize()
+            ms_ = []
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fb.jk_mixed_device(dD.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
+                e1.record(stream)
+                e1.synchronize()
+                ms_.append(e0.elapsed_time(e1))
+        tms = sum(ms_)
+        if ws > 1:
+            tms = max_over_ranks(tms, f"cuda:{device}")
+        mixed_builds[f"dD_scale_{scale:g}"] = {"builds_per_s": replica_rate(ws, args.steps, tms * 1e-3),
+                                                "ms_per_build": tms / args.steps}
 
     # --- per-class profile, roofline of the dominant class kernel.
     per_class_ms = fb.profile_build(Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
@@ -438,6 +477,10 @@ def run_gpu(args):
         "digest": {"bytes_per_build": 3 * n * n * 8,
                    "achieved_GBps": 3 * n * n * 8 / (tot_ms / args.steps * 1e-3) / 1e9,
                    "peak_GBps": hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm_peak else None},
+        # Fock builds/s of the mixed-precision incremental form on the same basis:
+        # the G of a density change dD = scale x the bench density (screened by
+        # Schwarz.|dD|, FP32 below 1e-7, accurate Boys function).
+        "mixed_incremental_builds": mixed_builds,
         "eri_shell_quartets_per_s": sq * value / ws, "eri_prim_quartets_per_s": pq * value / ws,
         "work": {"shell_quartets": sq, "prim_quartets": pq, "warp_tasks": wt},
         "per_class_ms": {c["class"]: round(t, 4) for c, t in zip(fl, per_class_ms) if t > 0},

@@ -128,3 +128,42 @@ def test_packed_layout_roundtrip():
     assert p[shells.packed_index(2, 5)] == A[2, 5]
     assert p[5 * 6 // 2 + 2] == A[2, 5]
     assert np.array_equal(shells.unpack(p, 7), A)
+
+
+def _replica_worker(rank, world, port, out):
+    import os
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+
+    # Each replica reports its own time; the job's time is the slowest one.
+    t = bench.max_over_ranks(1.0 + rank, "cpu")
+    out.put((rank, t, bench.replica_rate(world, 10, t)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_replicas_take_the_slowest_rank_gloo():
+    """bench.py --gpus N runs N independent replicas (the Fock build does not
+    shard here): every rank gets the maximum time, and the whole-job rate is
+    N x steps over it.  Two gloo ranks on the CPU."""
+    import random
+
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = random.randint(20000, 40000)
+    procs = [ctx.Process(target=_replica_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == [2.0, 2.0]
+    assert all(abs(r[2] - 10.0) < 1e-12 for r in res)
