@@ -99,10 +99,13 @@ def _class_tu(c, coop: bool) -> str:
             k = f"eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}>"
             sm = f"coop_smem_per_warp<{la}, {lb}, {lc}, {ld}, {pb}>() * sizeof(double) * DSS_COOP_WARPS"
             lines.append(f"  if (boys == {boys} && pure == {pure} && mixed == {mixed}) {{")
-            lines.append(f"    static bool attr = false;")
+            lines.append(f"    static bool attr[64] = {{}};  // per device: the attribute is per context")
+            lines.append(f"    int dev = 0;")
+            lines.append(f"    cudaGetDevice(&dev);")
             lines.append(f"    const size_t smem = {sm};")
-            lines.append(f"    if (!attr) {{ cudaFuncSetAttribute({k}, "
-                         f"cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }}")
+            lines.append(f"    if (dev < 0 || dev >= 64 || !attr[dev]) {{ cudaFuncSetAttribute({k}, "
+                         f"cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); "
+                         f"if (dev >= 0 && dev < 64) attr[dev] = true; }}")
             lines.append(f"    {k}<<<blocks, 32 * DSS_COOP_WARPS, smem, s>>>(a);")
             lines.append("  }")
         lines.append("}")

@@ -730,13 +730,18 @@ bool same_opts(const dss_scf_opts& a, const dss_scf_opts& c) {
 void launch_jacobi(dss_batch* b, const BatchView& v, int ka, int kv, int kt, int max_sweeps) {
   cudaStream_t s = b->ctx->stream;
   const int nb = (int)b->slot_mol.size();
-  static int optin = 0;
-  if (!optin) {
-    int dev = 0;
-    cudaGetDevice(&dev);
+  // Shared-memory opt-in per device (the function attribute is per context).
+  static int optin_dev[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int optin = 0;
+  if (dev >= 0 && dev < 64 && optin_dev[dev]) {
+    optin = optin_dev[dev];
+  } else {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncSetAttribute(k_jacobi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     cudaFuncSetAttribute(k_jacobi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (dev >= 0 && dev < 64) optin_dev[dev] = optin;
   }
   auto fits = [&](int nn_, bool vt) {
     return (dss_packed_size(nn_) + (vt ? (size_t)nn_ * nn_ : 0)) * 8 + dss_block_jacobi_smem(nn_) <= (size_t)optin;
