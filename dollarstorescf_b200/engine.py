@@ -224,6 +224,14 @@ class FockBuilder:
         self._check(self._L.dss_write_molden(self._h, path.encode(), sh.natom, _ip(Z), _dp(xyz),
                                              1 if write_virtual else 0))
 
+    def gradient(self, sh: ShellArrays, step: float = 1e-4) -> np.ndarray:
+        """Nuclear gradient [natom, 3] (hartree/bohr) of the last scf()/uhf()."""
+        Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
+        xyz = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
+        g = np.zeros(3 * sh.natom)
+        self._check(self._L.dss_gradient(self._h, sh.natom, _ip(Z), _dp(xyz), float(step), _dp(g)))
+        return g.reshape(sh.natom, 3)
+
     def sync(self) -> None:
         self._check(self._L.dss_sync(self._h))
 

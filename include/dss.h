@@ -231,6 +231,16 @@ int dss_scf_orbitals(const dss_ctx* ctx, int spin, double* C, double* eps);
 int dss_write_molden(dss_ctx* ctx, const char* path, int natom, const int* Z, const double* xyz_bohr,
                      int write_virtual);
 
+/* Nuclear gradient dE/dR (grad[3*natom], hartree/bohr) of the last
+ * dss_scf_solve / dss_uhf_solve, the quantity of scf::getEnergyGradient
+ * (chem/scf/Gradient.cpp:14-133, chem/scf/ExactCoulomb.cpp:125-195): the
+ * fixed-density energy tr(D H) + E_2e[D] - tr(W S) + V_nn (W the energy-weighted
+ * density of the final orbitals) differentiated by central differences of
+ * step bohr (1e-4 is a good choice) along each nuclear coordinate, each point a
+ * device one-electron evaluation and a device J/K build on displaced shells.
+ * Not an analytic derivative: O(step^2) truncation, 6 natom builds. */
+int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double* xyz_bohr, double step, double* grad);
+
 /* ---------------------------------------------------------------- batches of molecules */
 /* Many closed-shell molecules of uneven size solved together: each ERI class
  * is one launch over every molecule of the batch, and one SCF iteration of all

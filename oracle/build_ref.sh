@@ -49,6 +49,7 @@ SRCS="chem/GaussianIntegral.cpp chem/GTO.cpp chem/BasisReader.cpp chem/XYZReader
 chem/Molecule.cpp chem/Element.cpp chem/scf/SCFSolver.cpp chem/scf/SCFBasis.cpp
 chem/scf/SCFCommon.cpp chem/scf/SCFDIIS.cpp chem/scf/ExactCoulomb.cpp chem/scf/Energy.cpp
 chem/scf/Damping.cpp chem/scf/Population.cpp chem/scf/Output.cpp chem/scf/WriteOrbitals.cpp
+chem/scf/Gradient.cpp
 lalib/Lapack.cpp lalib/Complex.cpp lalib/PrintMatrix.cpp lalib/LBFGS.cpp
 util/FormattedStream.cpp util/TextReader.cpp util/TextUtil.cpp util/Time.cpp util/Parallel.cpp"
 OBJDIR="$SHADOW/obj"

@@ -32,6 +32,7 @@
 #include "chem/scf/SCFCommon.hpp"
 #include "chem/scf/SCFSolver.hpp"
 #include "chem/scf/WriteOrbitals.hpp"
+#include "chem/scf/Gradient.hpp"
 
 namespace flo {
 double boysFunctionExact(double x, uint m);
@@ -227,6 +228,18 @@ int ref_scf(double conv, double* E_total, double* D_alpha_packed, double* second
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   if (quiet) quiet_off();
   return (int)scf::iteration;
+}
+
+// Nuclear gradient dE/dR [natom*3] (hartree/bohr) at the last ref_scf's density
+// (scf::getEnergyGradient, chem/scf/Gradient.cpp:14-133).
+int ref_gradient(double* out, int quiet) {
+  if (!g_have_tensor) return -1;
+  if (quiet) quiet_on();
+  flo::VectorNd g;
+  scf::getEnergyGradient(g);
+  for (size_t i = 0; i < g.size(); ++i) out[i] = g[i];
+  if (quiet) quiet_off();
+  return (int)g.size();
 }
 
 // Molden file of the last ref_scf (scf::writeOrbitalsMolden, chem/scf/WriteOrbitals.cpp:17-137).

@@ -43,6 +43,8 @@ def lib():
         L.ref_scf.restype = ctypes.c_int
         L.ref_get_density.argtypes = [ctypes.c_int, dp]
         L.ref_write_molden.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        L.ref_gradient.argtypes = [dp, ctypes.c_int]
+        L.ref_gradient.restype = ctypes.c_int
         L.ref_electron_counts.argtypes = [ip, ip]
         L.ref_fock_2e.argtypes = [dp, dp]
         L.ref_fock_2e.restype = ctypes.c_int
@@ -100,6 +102,15 @@ def spin_density(spin: int) -> np.ndarray:
     D = np.zeros(n * (n + 1) // 2)
     L.ref_get_density(int(spin), _p(D))
     return D
+
+
+def gradient(natom: int) -> np.ndarray:
+    """The reference's nuclear gradient [natom, 3] at the last scf() density."""
+    g = np.zeros(3 * natom)
+    n = lib().ref_gradient(_p(g), 1)
+    if n < 0:
+        raise RuntimeError("reference state has no ERI tensor")
+    return g.reshape(natom, 3)
 
 
 def write_molden(path: str, write_virtual: bool = True) -> None:

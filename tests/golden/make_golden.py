@@ -10,6 +10,12 @@ oracle/build_ref.sh and driven through oracle/ref_harness.cpp:
   * <name>.molden  the reference's Molden files (scf::writeOrbitalsMolden, virtual
                    orbitals included) of water 6-31G* (RHF) and CH2 triplet
                    6-31G* (UHF) after converged solves
+  * <name>_grad.npz the nuclear gradient as the derivative of the reference's own
+                   converged total energy: a 4-point central difference (step
+                   1e-3 bohr, O(h^4)) over SCFs converged to 1e-12.  (The
+                   reference's scf::getEnergyGradient does not reproduce that
+                   derivative: for water 6-31G* it gives an asymmetric, several
+                   times larger gradient, and NaN for water STO-3G.)
   * <name>_uhf.npz open-shell molecules (multiplicity > 1, the reference's
                    unrestricted branch): charge, multiplicity, electron counts,
                    the converged energy and both final spin densities, S and H.
@@ -87,6 +93,36 @@ def write_uhf_case(name, mol, bas, pure, charge, mult) -> None:
     print(f"{name:18s} n={n:4d} na={na} nb={nb} E={E:.13f} it={it} ({secs:.2f}s)")
 
 
+def write_gradient_cases() -> None:
+    from dollarstorescf_b200.basis import Molecule
+
+    h = 1e-3
+    # Closed-shell molecules only: the reference's unrestricted solves of displaced
+    # open-shell geometries land on different states (the difference quotient of
+    # CH2 triplet breaks translational invariance by 0.17 Eh/bohr).
+    for name in ("water_631gs", "ch4_631g"):
+        d = np.load(os.path.join(HERE, name + ".npz"))
+        mol = Molecule([int(z) for z in d["Z"]], [tuple(p) for p in d["xyz"]])
+        mult = int(d["multiplicity"]) if "multiplicity" in d.files else 1
+        bas, pure = str(d["basis"]), bool(d["pure"])
+
+        def energy(a, k, delta):
+            xyz = [list(p) for p in mol.xyz]
+            xyz[a][k] += delta
+            sh = shells.build_shells(Molecule(list(mol.Z), [tuple(p) for p in xyz]), basis.builtin_basis(bas),
+                                     pure=pure)
+            refpy.setup(sh, multiplicity=mult)
+            return refpy.scf(1e-12)[0]
+
+        g = np.zeros((mol.natom, 3))
+        for a in range(mol.natom):
+            for k in range(3):
+                e = [energy(a, k, s * h) for s in (2, 1, -1, -2)]
+                g[a, k] = (-e[0] + 8.0 * e[1] - 8.0 * e[2] + e[3]) / (12.0 * h)
+        np.savez_compressed(os.path.join(HERE, name + "_grad.npz"), grad=g, step=h, stencil=4)
+        print(f"{name}_grad.npz", np.round(g, 8).tolist())
+
+
 def write_molden_cases() -> None:
     A = basis.molecule_from_angstrom
     for name, mol, bas, charge, mult in (
@@ -105,6 +141,11 @@ def main() -> None:
     if "molden" in only:
         write_molden_cases()
         only.discard("molden")
+        if not only:
+            return
+    if "gradient" in only:
+        write_gradient_cases()
+        only.discard("gradient")
         if not only:
             return
     if only:
@@ -126,6 +167,7 @@ def main() -> None:
     for name, mol, bas, pure, charge, mult in uhf_cases():
         write_uhf_case(name, mol, bas, pure, charge, mult)
     write_molden_cases()
+    write_gradient_cases()
 
 
 def write_case(name, mol, bas, pure, rng) -> None:
