@@ -78,8 +78,12 @@ def measure_rows(device: int, cpu_baseline: bool):
       uhf           CH2 triplet 6-31G* and the n-butyl radical 6-31G (doublet):
                     dss_uhf_solve from the core guess, conv 1e-10, vs the
                     reference's unrestricted solveMOs (ERI tensor + SCF).
+      gradient      water dimer 6-31G*: dss_gradient vs the time of the
+                    reference's gradient routine on the same converged state.
     """
     import time as _t
+
+    import numpy as np
 
     from dollarstorescf_b200 import basis as B
     from dollarstorescf_b200 import geometry, shells
@@ -144,6 +148,34 @@ def measure_rows(device: int, cpu_baseline: bool):
                 r["gpu_over_cpu"] = dtr / dt
         uhf[name] = r
     out["uhf"] = uhf
+
+    # Nuclear gradient (dss_gradient: 6 natom device builds on displaced shells)
+    # of a converged water dimer 6-31G*, beside the reference's gradient routine
+    # on the same converged state (its values differ from the derivative of its
+    # own energy, so only the time compares).
+    dimer = geometry.water_dimer(0)
+    shd = shells.build_shells(dimer, B.builtin_basis("6-31G*"), pure=True)
+    gr = {"workload": "(H2O)2 RHF/6-31G* (36 functions, 6 nuclei)"}
+    with FockBuilder(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as fb:
+        fb.set_basis(shd)
+        S, T, V, en = fb.one_electron(shd)
+        fb.scf(T + V, S, shd.n_electrons() // 2, en, conv=1e-10)
+        fb.gradient(shd)
+        t0 = _t.perf_counter()
+        g = fb.gradient(shd)
+        gr["gpu_s"] = _t.perf_counter() - t0
+        gr["max_abs_net_force"] = float(np.abs(g.sum(axis=0)).max())
+    if cpu_baseline:
+        from oracle import refpy
+
+        if refpy.available():
+            refpy.setup(shd)
+            refpy.scf(1e-10)
+            t0 = _t.perf_counter()
+            refpy.gradient(shd.natom)
+            gr["cpu_baseline"] = {"seconds": _t.perf_counter() - t0, "cores": 1, "kind": "reference",
+                                  "sample": "scf::getEnergyGradient on the same converged state"}
+    out["gradient"] = gr
     return out
 
 
