@@ -548,6 +548,22 @@ struct dss_batch_mol {
   BasisHost basis;  // molecule-local
   PairSet pairs;    // its shell pairs and Schwarz factors, made once at admission
   bool needs_x = true;  // X = S^-1/2 not computed yet (done for all new molecules at the next step)
+  long long pp_off = 0;  // its primitive pairs' first record in the batch's device pool
+};
+
+// Device pool of the live molecules' primitive-pair records (10 doubles each),
+// filled at admission, so a change of composition moves no primitive pairs:
+// the merged pair list indexes the pool.  Removal leaves a hole; the pool is
+// compacted when it grows.
+struct PpPool {
+  double* ptr = nullptr;
+  size_t cap = 0, used = 0;  // records
+  PpPool() = default;
+  PpPool(const PpPool&) = delete;
+  PpPool& operator=(const PpPool&) = delete;
+  ~PpPool() {
+    if (ptr) cudaFree(ptr);
+  }
 };
 
 struct dss_batch {
@@ -565,6 +581,7 @@ struct dss_batch {
   DevBuf<int> d_n, d_active, d_active_next, d_nact;
   DevBuf<int> d_pending;  // per slot: 1 while the molecule's X is not computed
   DevBuf<double> admit_tmp;  // admission scratch (packed H, S, guess), grow-only
+  PpPool pp_pool;
   int nmax = 0;
   int* h_nact = nullptr;  // pinned: molecules still iterating, molecules finished in the last iteration
   std::vector<int> last_finished;  // handles whose results the last dss_batch_step produced
@@ -620,6 +637,49 @@ BatchView view(dss_batch* b, const int* active) {
   v.nb = (int)b->slot_mol.size();
   v.ds = b->ds;
   return v;
+}
+
+// Uploads a new molecule's primitive pairs into the pool (growing and compacting
+// it over the live molecules when full) and records their offset.
+int pool_put(dss_batch* b, dss_batch_mol* m) {
+  PpPool& pool = b->pp_pool;
+  cudaStream_t s = b->ctx->stream;
+  const size_t rec = m->pairs.pp.size() / 10;
+  if (pool.used + rec > pool.cap) {
+    size_t live = rec;
+    for (const auto& o : b->mols)
+      if (o.live) live += o.pairs.pp.size() / 10;
+    const size_t cap = std::max<size_t>(std::max<size_t>(2 * pool.cap, live + live / 2), 1 << 16);
+    double* np = nullptr;
+    if (cudaMalloc((void**)&np, cap * 10 * sizeof(double)) != cudaSuccess) return DSS_ERR_OOM;
+    size_t at = 0;
+    for (auto& o : b->mols) {
+      if (!o.live) continue;
+      const size_t r = o.pairs.pp.size() / 10;
+      if (r && cudaMemcpyAsync(np + at * 10, pool.ptr + (size_t)o.pp_off * 10, r * 10 * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        cudaFree(np);
+        return DSS_ERR_CUDA;
+      }
+      o.pp_off = (long long)at;
+      at += r;
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      cudaFree(np);
+      return DSS_ERR_CUDA;
+    }
+    if (pool.ptr) cudaFree(pool.ptr);
+    pool.ptr = np;
+    pool.cap = cap;
+    pool.used = at;
+    b->dirty = true;  // the live molecules' offsets moved
+  }
+  if (rec && cudaMemcpyAsync(pool.ptr + pool.used * 10, m->pairs.pp.data(), rec * 10 * sizeof(double),
+                             cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return DSS_ERR_CUDA;
+  m->pp_off = (long long)pool.used;
+  pool.used += rec;
+  return DSS_OK;
 }
 
 // Rebuilds the batch basis (pairs, Schwarz factors, work lists) and the
@@ -686,8 +746,45 @@ int rebuild(dss_batch* b) {
     off += (int)b->mols[b->slot_mol[s]].basis.l.size();
   }
   PairSet P;
-  dss_pairs_merge(parts, shell_off, &P);
-  int rc = dss_pairs_install(ctx, std::move(B), std::move(P));
+  std::vector<long long> pp_off(nb);
+  for (int sl = 0; sl < nb; ++sl) pp_off[sl] = b->mols[b->slot_mol[sl]].pp_off;
+  dss_pairs_merge(parts, shell_off, &P, &pp_off);
+  ctx->ext_pp = reinterpret_cast<const PrimPair*>(b->pp_pool.ptr);
+  // Work lists: every molecule's own lists (made at admission), their pair
+  // indices moved to the merged (class, molecule) order: no search over the
+  // batch's pairs when its composition changes.
+  const int ncls = dss_num_pair_classes();
+  std::vector<std::vector<int>> lc0(nb), lc1(nb);
+  std::vector<int> mc0(ncls, 0);
+  std::vector<std::vector<int>> off(nb, std::vector<int>(ncls, 0));
+  for (int sl = 0; sl < nb; ++sl) dss_class_ranges(parts[sl]->cls, &lc0[sl], &lc1[sl]);
+  for (int c = 0, acc = 0; c < ncls; ++c) {
+    mc0[c] = acc;
+    for (int sl = 0; sl < nb; ++sl) {
+      off[sl][c] = acc - mc0[c];
+      acc += lc1[sl][c] - lc0[sl][c];
+    }
+  }
+  HostTasks merged;
+  const size_t nq = parts.empty() ? 0 : parts[0]->tasks.tasks.size();
+  merged.tasks.assign(nq, {});
+  merged.shell_quartets.assign(nq, 0);
+  merged.prim_quartets.assign(nq, 0);
+  for (size_t ci = 0; ci < nq; ++ci) {
+    const int bc = dss_quartet_bra_class((int)ci), kc = dss_quartet_ket_class((int)ci);
+    size_t cnt = 0;
+    for (int sl = 0; sl < nb; ++sl) cnt += parts[sl]->tasks.tasks[ci].size();
+    std::vector<int4>& out = merged.tasks[ci];
+    out.reserve(cnt);
+    for (int sl = 0; sl < nb; ++sl) {
+      const HostTasks& ht = parts[sl]->tasks;
+      const int db = mc0[bc] + off[sl][bc] - lc0[sl][bc], dk = mc0[kc] + off[sl][kc] - lc0[sl][kc];
+      for (const int4& t : ht.tasks[ci]) out.push_back(make_int4(t.x + db, t.y + dk, t.z, sl));
+      merged.shell_quartets[ci] += ht.shell_quartets[ci];
+      merged.prim_quartets[ci] += ht.prim_quartets[ci];
+    }
+  }
+  int rc = dss_pairs_install(ctx, std::move(B), std::move(P), &merged);
   if (rc != DSS_OK) return bfail(b, rc, ctx->err);
   ctx->nbf = 1;  // batch mode: accumulators are addressed per molecule
   if (ctx->d_dmax.resize((size_t)std::max<long long>(dtot, 1)) != cudaSuccess)
@@ -1004,8 +1101,10 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   const size_t np = (size_t)m.n * (m.n + 1) / 2;
   const double e_nuc = dss_nuclear_repulsion(natom, Z, xyz);
   cudaSetDevice(b->ctx->opts.device);
-  rc = dss_pairs_make(b->ctx, m.basis, &m.pairs);
+  rc = dss_pairs_make(b->ctx, m.basis, &m.pairs, true);  // with its own work lists
   if (rc != DSS_OK) return bfail(b, rc, std::string("dss_batch_add: shell pairs: ") + b->ctx->err);
+  rc = pool_put(b, &m);
+  if (rc != DSS_OK) return bfail(b, rc, "dss_batch_add: primitive-pair pool allocation failed");
   m.size = region_size(m.n, b->ds);
   size_t off = 0;
   if (!arena_alloc(b, m.size, &off))

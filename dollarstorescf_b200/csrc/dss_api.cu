@@ -321,7 +321,7 @@ int dss_build_jk(dss_ctx* ctx, const double* Dp, double* Jp, double* Kp) {
 // ------------------------------------------------------------------ pairs, Schwarz, tasks
 static_assert(sizeof(PrimPair) == 10 * sizeof(double), "PairSet stores primitive pairs as 10 doubles");
 
-int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out) {
+int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out, bool with_tasks) {
   const int ns = (int)B.l.size();
   // Unordered shell pairs {a, b} inside one molecule; stored with l_a >= l_b (ties: a >= b).
   struct PairTmp {
@@ -455,16 +455,23 @@ int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out) {
     if (pn[o]) std::memcpy(P.pp.data() + off * 10, &pp[p0[o]], (size_t)pn[o] * sizeof(PrimPair));
     off += pn[o];
   }
+  if (with_tasks) {
+    std::vector<int> c0, c1, mol0(np, 0);
+    dss_class_ranges(P.cls, &c0, &c1);
+    dss_make_tasks(c0, c1, P.Q, P.pn, mol0, 1, ctx->opts.schwarz_threshold, &P.tasks);
+    P.have_tasks = true;
+  }
   return DSS_OK;
 }
 
-void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out) {
+void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out,
+                     const std::vector<long long>* pp_offset) {
   PairSet& P = *out;
   P = PairSet();
   size_t np = 0, npp = 0;
   for (const PairSet* s : parts) {
     np += s->pa.size();
-    npp += s->pp.size();
+    if (!pp_offset) npp += s->pp.size();
   }
   P.pa.reserve(np);
   P.pb.reserve(np);
@@ -476,8 +483,12 @@ void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector
   P.pp.reserve(npp);
   std::vector<int> pp_off(parts.size()), cur(parts.size(), 0);
   for (size_t m = 0; m < parts.size(); ++m) {
-    pp_off[m] = (int)(P.pp.size() / 10);
-    P.pp.insert(P.pp.end(), parts[m]->pp.begin(), parts[m]->pp.end());
+    if (pp_offset) {
+      pp_off[m] = (int)(*pp_offset)[m];
+    } else {
+      pp_off[m] = (int)(P.pp.size() / 10);
+      P.pp.insert(P.pp.end(), parts[m]->pp.begin(), parts[m]->pp.end());
+    }
   }
   // Each part is sorted by class first: walking the classes in order and taking
   // every part's run of that class gives the (class, molecule, ...) order.
@@ -497,7 +508,7 @@ void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector
     }
 }
 
-int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P) {
+int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks) {
   const int np = (int)P.pa.size();
   ctx->nbf = B.nbf;
   ctx->pure = B.pure;
@@ -538,6 +549,7 @@ int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P) {
   ctx->class_pair0 = c0;
   ctx->class_pair1 = c1;
   ctx->basis = std::move(B);
+  if (tasks) return dss_install_tasks(ctx, *tasks);
   return dss_build_tasks(ctx);
 }
 
@@ -548,12 +560,36 @@ int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B) {
   return dss_pairs_install(ctx, std::move(B), std::move(P));
 }
 
-int dss_build_tasks(dss_ctx* ctx) {
+void dss_class_ranges(const std::vector<int>& cls, std::vector<int>* c0, std::vector<int>* c1) {
   const int ncls = DSS_N_PAIR_CLASSES;
-  const double thr = ctx->opts.schwarz_threshold;
-  const std::vector<double>& Q = ctx->h_Q;
-  const std::vector<int>& npp = ctx->h_pair_npp;
-  const std::vector<int>& pmol = ctx->h_pair_mol;
+  const int np = (int)cls.size();
+  c0->assign(ncls, 0);
+  c1->assign(ncls, 0);
+  for (int c = 0, q = 0; c < ncls; ++c) {
+    (*c0)[c] = q;
+    while (q < np && cls[q] == c) ++q;
+    (*c1)[c] = q;
+  }
+}
+
+namespace {
+struct QuartetClassInfo {
+  int la, lb, lc, ld, bc, kc;
+};
+const QuartetClassInfo kQuartetClasses[] = {
+#define DSS_CLASS_ROW(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_, e_, f_},
+    DSS_FOR_EACH_CLASS(DSS_CLASS_ROW)
+#undef DSS_CLASS_ROW
+};
+}  // namespace
+
+int dss_num_pair_classes() { return DSS_N_PAIR_CLASSES; }
+int dss_quartet_bra_class(int i) { return kQuartetClasses[i].bc; }
+int dss_quartet_ket_class(int i) { return kQuartetClasses[i].kc; }
+
+void dss_make_tasks(const std::vector<int>& c0, const std::vector<int>& c1, const std::vector<double>& Q,
+                    const std::vector<int>& npp, const std::vector<int>& pmol, int nmol, double thr, HostTasks* out) {
+  const int ncls = DSS_N_PAIR_CLASSES;
   // Groups per class: [g0, g1) ranges of one molecule with equal npp; per class
   // and molecule the range of its groups.
   struct Group {
@@ -561,13 +597,13 @@ int dss_build_tasks(dss_ctx* ctx) {
   };
   std::vector<std::vector<Group>> groups(ncls);
   std::vector<std::vector<std::pair<int, int>>> mol_groups(ncls);
-  const int nm = ctx->nmol > 0 ? ctx->nmol : 1;
+  const int nm = nmol > 0 ? nmol : 1;
   for (int c = 0; c < ncls; ++c) {
     mol_groups[c].assign(nm, {0, 0});
-    int q = ctx->class_pair0[c];
-    while (q < ctx->class_pair1[c]) {
+    int q = c0[c];
+    while (q < c1[c]) {
       int e = q;
-      while (e < ctx->class_pair1[c] && npp[e] == npp[q] && pmol[e] == pmol[q]) ++e;
+      while (e < c1[c] && npp[e] == npp[q] && pmol[e] == pmol[q]) ++e;
       const int m = pmol[q];
       if (mol_groups[c][m].second == 0) mol_groups[c][m] = {(int)groups[c].size(), (int)groups[c].size()};
       groups[c].push_back({q, e, m});
@@ -575,35 +611,14 @@ int dss_build_tasks(dss_ctx* ctx) {
       q = e;
     }
   }
-  // The previous work-list buffers are reused (grow-only) by the new lists.
-  std::vector<ClassTasks> old = std::move(ctx->tasks);
-  ctx->tasks.clear();
-  ctx->n_shell_quartets = 0;
-  ctx->n_prim_quartets = 0;
-  ctx->n_warp_tasks = 0;
-  struct ClassInfo {
-    int la, lb, lc, ld, bc, kc;
-  };
-  static const ClassInfo kClasses[] = {
-#define DSS_CLASS_ROW(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_, e_, f_},
-      DSS_FOR_EACH_CLASS(DSS_CLASS_ROW)
-#undef DSS_CLASS_ROW
-  };
-  for (const ClassInfo& ci : kClasses) {
-    const int bc = ci.bc, kc = ci.kc;
-    ClassTasks ct;
-    if (ctx->tasks.size() < old.size()) ct.d_tasks = std::move(old[ctx->tasks.size()].d_tasks);
-    ct.la = ci.la;
-    ct.lb = ci.lb;
-    ct.lc = ci.lc;
-    ct.ld = ci.ld;
-    const size_t idx = ctx->tasks.size();
-    if (idx < ctx->class_variant.size() && ctx->class_variant[idx] >= 0)
-      ct.variant = ctx->class_variant[idx];
-    else
-      ct.variant = dss_has_coop(ci.la, ci.lb, ci.lc, ci.ld) ? 1 : 0;
-    std::vector<int4> h;
-    for (int ib = ctx->class_pair0[bc]; ib < ctx->class_pair1[bc]; ++ib) {
+  const int nq = (int)(sizeof(kQuartetClasses) / sizeof(kQuartetClasses[0]));
+  out->tasks.assign(nq, {});
+  out->shell_quartets.assign(nq, 0);
+  out->prim_quartets.assign(nq, 0);
+  for (int ci = 0; ci < nq; ++ci) {
+    const int bc = kQuartetClasses[ci].bc, kc = kQuartetClasses[ci].kc;
+    std::vector<int4>& h = out->tasks[ci];
+    for (int ib = c0[bc]; ib < c1[bc]; ++ib) {
       const double Qb = Q[ib];
       const std::pair<int, int> gr = mol_groups[kc][pmol[ib]];
       for (int gi = gr.first; gi < gr.second; ++gi) {
@@ -622,21 +637,53 @@ int dss_build_tasks(dss_ctx* ctx) {
         for (int k0 = 0; k0 < nvalid; k0 += 32) {
           const int cnt = std::min(32, nvalid - k0);
           h.push_back(make_int4(ib, g.g0 + k0, cnt, pmol[ib]));
-          ct.shell_quartets += cnt;
-          ct.prim_quartets += (long long)cnt * npp[ib] * npp[g.g0];
+          out->shell_quartets[ci] += cnt;
+          out->prim_quartets[ci] += (long long)cnt * npp[ib] * npp[g.g0];
         }
       }
     }
-    ct.ntasks = (int)h.size();
+  }
+}
+
+int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
+  // The previous work-list buffers are reused (grow-only) by the new lists.
+  std::vector<ClassTasks> old = std::move(ctx->tasks);
+  ctx->tasks.clear();
+  ctx->n_shell_quartets = 0;
+  ctx->n_prim_quartets = 0;
+  ctx->n_warp_tasks = 0;
+  const int nq = (int)(sizeof(kQuartetClasses) / sizeof(kQuartetClasses[0]));
+  for (int idx = 0; idx < nq; ++idx) {
+    const QuartetClassInfo& ci = kQuartetClasses[idx];
+    ClassTasks ct;
+    if ((size_t)idx < old.size()) ct.d_tasks = std::move(old[idx].d_tasks);
+    ct.la = ci.la;
+    ct.lb = ci.lb;
+    ct.lc = ci.lc;
+    ct.ld = ci.ld;
+    if ((size_t)idx < ctx->class_variant.size() && ctx->class_variant[idx] >= 0)
+      ct.variant = ctx->class_variant[idx];
+    else
+      ct.variant = dss_has_coop(ci.la, ci.lb, ci.lc, ci.ld) ? 1 : 0;
+    ct.ntasks = (int)ht.tasks[idx].size();
+    ct.shell_quartets = ht.shell_quartets[idx];
+    ct.prim_quartets = ht.prim_quartets[idx];
     ctx->n_warp_tasks += ct.ntasks;
     ctx->n_shell_quartets += ct.shell_quartets;
     ctx->n_prim_quartets += ct.prim_quartets;
     ctx->tasks.push_back(std::move(ct));
-    int rc_ = upload(ctx, ctx->tasks.back().d_tasks, h);
+    int rc_ = upload(ctx, ctx->tasks.back().d_tasks, ht.tasks[idx]);
     if (rc_ != DSS_OK) return rc_;
   }
   DSS_CUDA(cudaStreamSynchronize(ctx->stream));
   return DSS_OK;
+}
+
+int dss_build_tasks(dss_ctx* ctx) {
+  HostTasks ht;
+  dss_make_tasks(ctx->class_pair0, ctx->class_pair1, ctx->h_Q, ctx->h_pair_npp, ctx->h_pair_mol, ctx->nmol,
+                 ctx->opts.schwarz_threshold, &ht);
+  return dss_install_tasks(ctx, ht);
 }
 
 int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events,
@@ -692,7 +739,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.pair_b = ctx->d_pair_b.ptr;
     a.pair_pp0 = ctx->d_pair_pp0.ptr;
     a.pair_npp = ctx->d_pair_npp.ptr;
-    a.pp = ctx->d_pp.ptr;
+    a.pp = ctx->ext_pp ? ctx->ext_pp : ctx->d_pp.ptr;
     a.sh_xyz = ctx->d_sh_xyz.ptr;
     a.sh_f0 = ctx->d_sh_f0.ptr;
     a.D = D;

@@ -98,6 +98,7 @@ struct dss_ctx {
   int nbf = 0, pure = 1, nshell = 0;
   BasisHost basis;
   DevBuf<PrimPair> d_pp;
+  const PrimPair* ext_pp = nullptr;  // batch mode: the batch's device pool of primitive pairs (used instead of d_pp)
   DevBuf<int> d_pair_a, d_pair_b, d_pair_pp0, d_pair_npp, d_sh_f0;
   DevBuf<double> d_sh_xyz, d_Q, d_Qs;  // Schwarz factors: computation order, sorted pair order
   DevBuf<int> d_sh_nf;                  // functions per shell
@@ -176,18 +177,34 @@ cudaError_t dss_boys_cell_table(const double** out);
 int dss_cuda_check(dss_ctx* ctx, cudaError_t e, const char* what);
 // Shell pairs of a basis with their primitive pairs and Schwarz factors, sorted
 // by (pair class, molecule, primitive-pair count descending, Q descending).
+// Work lists of a pair set on the host, per quartet class (DSS_FOR_EACH_CLASS
+// order): warp tasks {bra pair, first ket pair, ket count, molecule} and the
+// shell / primitive quartets they cover.
+struct HostTasks {
+  std::vector<std::vector<int4>> tasks;
+  std::vector<long long> shell_quartets, prim_quartets;
+};
+
 struct PairSet {
   std::vector<int> pa, pb, p0, pn, cls, mol;  // shells, first primitive pair, primitive pairs, class, molecule
   std::vector<double> Q;
   std::vector<double> pp;  // primitive pairs, 10 doubles each (the PrimPair record)
+  // Batch molecules: the molecule's own work lists (pair indices local to this
+  // set, molecule 0), made once at admission and offset into a batch's lists.
+  HostTasks tasks;
+  bool have_tasks = false;
 };
 // Pairs of one basis (Schwarz factors computed on the device, synchronously).
-int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out);
+int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out, bool with_tasks = false);
 // Concatenation of per-molecule pair sets in batch order: part m's shells start
 // at shell_offset[m] and its pairs become molecule m's.
-void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out);
+// pp_offset (optional): each part's primitive pairs already sit on the device
+// at that record offset of one pool; the merged set then carries no pp records
+// and its p0 index that pool.
+void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out,
+                     const std::vector<long long>* pp_offset = nullptr);
 // Makes B and P the context's basis: uploads, class ranges, work lists.
-int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P);
+int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks = nullptr);
 int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
 // Shells from the C-ABI arrays: validation and the reference's primitive normalisation.
 int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,
@@ -204,6 +221,19 @@ int dss_one_electron_basis(cudaStream_t s, const BasisHost& B, int natom, const 
 // sum_{A<B} Z_A Z_B / R_AB.
 double dss_nuclear_repulsion(int natom, const int* Z, const double* xyz);
 int dss_build_tasks(dss_ctx* ctx);
+// Work lists for pairs sorted by (class, molecule, npp, Q): class ranges
+// [c0[c], c1[c]), Schwarz factors, primitive-pair counts and molecules.
+void dss_make_tasks(const std::vector<int>& c0, const std::vector<int>& c1, const std::vector<double>& Q,
+                    const std::vector<int>& npp, const std::vector<int>& pmol, int nmol, double thr, HostTasks* out);
+// Uploads work lists as the context's (device buffers reused, grow-only).
+int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht);
+// Number of shell-pair classes; bra and ket pair classes of quartet class i
+// (DSS_FOR_EACH_CLASS order).
+int dss_num_pair_classes();
+int dss_quartet_bra_class(int i);
+int dss_quartet_ket_class(int i);
+// Per-class pair ranges of a pair set.
+void dss_class_ranges(const std::vector<int>& cls, std::vector<int>* c0, std::vector<int>* c1);
 // G = (Jacc + Jacc^T) - (Kacc + Kacc^T) / 2, dense n x n.
 void dss_symmetrize_combine(cudaStream_t s, int n, const double* Jacc, const double* Kacc, double* G);
 // How one J/K accumulation runs: Boys mode and, for the mixed-precision form,
