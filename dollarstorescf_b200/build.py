@@ -79,7 +79,7 @@ def _class_tu(c, coop: bool) -> str:
     if (la, lb) == (lc, ld):
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s) {{")
         lines.append("  const int threads = 128;")
-        lines.append("  const unsigned blocks = (unsigned)((a.npair + threads - 1) / threads);")
+        lines.append("  const unsigned blocks = (unsigned)(((long long)a.npair * 32 + threads - 1) / threads);")
         lines.append("  if (!blocks) return;")
         for boys in (0, 1):
             for pure in (1, 0):

@@ -331,28 +331,37 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
   }
 }
 
-// Schwarz factors Q_ab = sqrt(max_ij |(ij|ij)|) for the pairs of one class.
+// Schwarz factors Q_ab = sqrt(max_ij |(ij|ij)|) for the pairs of one class: one
+// warp per shell pair, the lanes splitting the bra primitive pairs (each lane
+// sums its bra primitive pairs against every ket primitive pair), the diagonal
+// integrals summed across the warp.
 template <int LA, int LB, int BOYS, bool PURE>
 __global__ void __launch_bounds__(128) schwarz_kernel(SchwarzArgs a) {
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= a.npair) return;
-  const int pr = a.pair0 + idx;
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= a.npair) return;
+  const int pr = a.pair0 + w;
   const int sa = a.pair_a[pr], sb = a.pair_b[pr];
   const double ABx = a.sh_xyz[3 * sa] - a.sh_xyz[3 * sb];
   const double ABy = a.sh_xyz[3 * sa + 1] - a.sh_xyz[3 * sb + 1];
   const double ABz = a.sh_xyz[3 * sa + 2] - a.sh_xyz[3 * sb + 2];
   const PrimPair* pp = a.pp + a.pair_pp0[pr];
   const int npp = a.pair_npp[pr];
-  double I[NA * NB * NA * NB];
-  EriClass<LA, LB, LA, LB>::template eval<BOYS, PURE>(pp, npp, pp, npp, ABx, ABy, ABz, ABx, ABy, ABz, I,
-                                                      a.boys_cell);
+  double diag[NA * NB];
+#pragma unroll
+  for (int q = 0; q < NA * NB; ++q) diag[q] = 0.0;
+  for (int ib = lane; ib < npp; ib += 32) {
+    double I[NA * NB * NA * NB];
+    EriClass<LA, LB, LA, LB>::template eval<BOYS, PURE>(pp + ib, 1, pp, npp, ABx, ABy, ABz, ABx, ABy, ABz, I,
+                                                        a.boys_cell);
+#pragma unroll
+    for (int q = 0; q < NA * NB; ++q) diag[q] += I[q * NA * NB + q];
+  }
   double mx = 0.0;
 #pragma unroll
-  for (int i = 0; i < NA; ++i)
-#pragma unroll
-    for (int j = 0; j < NB; ++j) mx = fmax(mx, fabs(I[((i * NB + j) * NA + i) * NB + j]));
-  a.Q[pr] = sqrt(mx);
+  for (int q = 0; q < NA * NB; ++q) mx = fmax(mx, fabs(warp_sum(diag[q])));
+  if (lane == 0) a.Q[pr] = sqrt(mx);
 }
 
 // Host-side launchers (one translation unit per class defines them).
