@@ -110,6 +110,12 @@ def load():
     L.dss_scf_orbitals.restype = ctypes.c_int
     L.dss_write_molden.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ip, dp, ctypes.c_int]
     L.dss_write_molden.restype = ctypes.c_int
+    L.dss_write_wfx.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ip, dp, ctypes.c_int]
+    L.dss_write_wfx.restype = ctypes.c_int
+    L.dss_save_density.argtypes = [vp, ctypes.c_char_p]
+    L.dss_save_density.restype = ctypes.c_int
+    L.dss_load_density.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ip, ip, ip, dp, dp]
+    L.dss_load_density.restype = ctypes.c_int
     L.dss_gradient.argtypes = [vp, ctypes.c_int, ip, dp, ctypes.c_double, dp]
     L.dss_gradient.restype = ctypes.c_int
     L.dss_build_jk_device_noalloc.argtypes = [vp, vp, vp, vp]

@@ -224,6 +224,22 @@ class FockBuilder:
         self._check(self._L.dss_write_molden(self._h, path.encode(), sh.natom, _ip(Z), _dp(xyz),
                                              1 if write_virtual else 0))
 
+    def write_wfx(self, path: str, sh: ShellArrays, write_virtual: bool = True) -> None:
+        """WFX file of the last scf()/uhf() (scf::writeOrbitalsWFX)."""
+        Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
+        xyz = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
+        self._check(self._L.dss_write_wfx(self._h, path.encode(), sh.natom, _ip(Z), _dp(xyz),
+                                          1 if write_virtual else 0))
+
+    def save_density(self, path: str) -> None:
+        """Density checkpoint of the last scf()/uhf() (restart file)."""
+        self._check(self._L.dss_save_density(self._h, path.encode()))
+
+    def load_density(self, path: str) -> Tuple[np.ndarray, np.ndarray, int, int, int]:
+        """(D_alpha, D_beta (packed-U), spins, n_alpha, n_beta) of a density
+        checkpoint for the current basis; usable as scf()/uhf() guesses."""
+        return load_density(path, self.nbf, self)
+
     def gradient(self, sh: ShellArrays, step: float = 1e-4) -> np.ndarray:
         """Nuclear gradient [natom, 3] (hartree/bohr) of the last scf()/uhf()."""
         Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
@@ -239,3 +255,19 @@ class FockBuilder:
         a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self._check(self._L.dss_work_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
+
+
+def load_density(path: str, nbf: int, fb: Optional["FockBuilder"] = None):
+    """Reads a density checkpoint written by FockBuilder.save_density (host
+    only): (D_alpha, D_beta (packed-U), spins, n_alpha, n_beta)."""
+    L = _lib.load()
+    np_ = nbf * (nbf + 1) // 2
+    Da = np.zeros(np_)
+    Db = np.zeros(np_)
+    sp, na, nb = (ctypes.c_int(0) for _ in range(3))
+    rc = L.dss_load_density(fb._h if fb is not None else None, path.encode(), int(nbf), ctypes.byref(sp),
+                            ctypes.byref(na), ctypes.byref(nb), _dp(Da), _dp(Db))
+    if rc != 0:
+        msg = L.dss_last_error(fb._h).decode() if fb is not None else "dss_load_density failed"
+        raise _lib.DssError(rc, msg)
+    return Da, Db, sp.value, na.value, nb.value

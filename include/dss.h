@@ -231,6 +231,32 @@ int dss_scf_orbitals(const dss_ctx* ctx, int spin, double* C, double* eps);
 int dss_write_molden(dss_ctx* ctx, const char* path, int natom, const int* Z, const double* xyz_bohr,
                      int write_virtual);
 
+/* WFX file of the last solve, replacing scf::writeOrbitalsWFX
+ * (chem/scf/WriteOrbitals.cpp:139-458): the same sections (nuclei, electron
+ * counts, Cartesian primitives per atom in WFX type order, occupations,
+ * energies, spin types, orbital coefficients on the primitives), all orbitals
+ * when write_virtual, else the occupied ones, alpha then beta.  Beta
+ * occupations count the beta electrons (the reference's loop counts alpha
+ * electrons there, WriteOrbitals.cpp:350).  5D bases, l <= 2. */
+int dss_write_wfx(dss_ctx* ctx, const char* path, int natom, const int* Z, const double* xyz_bohr,
+                  int write_virtual);
+
+/* Density checkpoint (restart file) of the last dss_scf_solve / dss_uhf_solve:
+ * the spin densities (packed-U; D_alpha only for a restricted solve), the
+ * electron counts and a checksum.  The reference has no restart file of its
+ * own (chem/scf/WriteOrbitals.cpp writes viewer output only); the file feeds
+ * the guess of a later solve (dss_scf_opts.use_guess). */
+int dss_save_density(dss_ctx* ctx, const char* path);
+
+/* Reads a density checkpoint for a basis of nbf functions into D_alpha and (if
+ * not NULL) D_beta (a restricted file gives D_beta = D_alpha); *spins,
+ * *n_alpha, *n_beta (each optional) receive the file's spin count and electron
+ * counts.  Host only.  Rejects a file of another basis size, a truncated file
+ * and a checksum mismatch (DSS_ERR_INVALID; the message goes to ctx, which may
+ * be NULL). */
+int dss_load_density(dss_ctx* ctx, const char* path, int nbf, int* spins, int* n_alpha, int* n_beta,
+                     double* D_alpha, double* D_beta);
+
 /* Nuclear gradient dE/dR (grad[3*natom], hartree/bohr) of the last
  * dss_scf_solve / dss_uhf_solve, the quantity of scf::getEnergyGradient
  * (chem/scf/Gradient.cpp:14-133, chem/scf/ExactCoulomb.cpp:125-195): the

@@ -298,14 +298,19 @@ def _diis_ring(B, errs, focks, e, Fnew, diis_size):
 
 
 def scf_uhf(S: np.ndarray, H: np.ndarray, eri: np.ndarray, n_alpha: int, n_beta: int, e_nuc: float,
-            conv: float = 1e-10, diis_size: int = 8, max_iter: int = 500):
+            conv: float = 1e-10, diis_size: int = 8, max_iter: int = 500, guess=None):
     """The reference's unrestricted loop restated (chem/scf/SCFSolver.cpp:120-172,
     196-237; one DIIS solver per spin, chem/scf/SCFDIIS.cpp:14-52; final energy
-    chem/scf/Energy.cpp:21-50).  Returns (E_total, D_alpha, D_beta, iterations)."""
+    chem/scf/Energy.cpp:21-50).  Returns (E_total, D_alpha, D_beta, iterations).
+    guess: optional dense (D_alpha, D_beta) that replaces the core guess (zero
+    densities) as the start of the same loop, the restart of a checkpoint."""
     n = S.shape[0]
     s, U = np.linalg.eigh(S)
     X = (U * (1.0 / np.sqrt(s))) @ U.T
-    D = [np.zeros((n, n)), np.zeros((n, n))]
+    if guess is None:
+        D = [np.zeros((n, n)), np.zeros((n, n))]
+    else:
+        D = [np.array(guess[0], dtype=float), np.array(guess[1], dtype=float)]
     nocc = (n_alpha, n_beta)
     E = 0.0
     E_prev = 0.0

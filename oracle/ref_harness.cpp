@@ -249,6 +249,13 @@ void ref_write_molden(const char* path, int write_virtual, int quiet) {
   if (quiet) quiet_off();
 }
 
+// WFX file of the last ref_scf (scf::writeOrbitalsWFX, chem/scf/WriteOrbitals.cpp:139-458).
+void ref_write_wfx(const char* path, int write_virtual, int quiet) {
+  if (quiet) quiet_on();
+  scf::writeOrbitalsWFX(std::string(path), write_virtual != 0);
+  if (quiet) quiet_off();
+}
+
 // Spin density (0 = alpha, 1 = beta; packed-U) after ref_scf, and the
 // electron counts scf::assignMolecule derived from charge and multiplicity.
 void ref_get_density(int spin, double* D_packed) { copy_packed(scf::density_matrix[spin ? 1 : 0], D_packed); }

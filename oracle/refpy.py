@@ -43,6 +43,7 @@ def lib():
         L.ref_scf.restype = ctypes.c_int
         L.ref_get_density.argtypes = [ctypes.c_int, dp]
         L.ref_write_molden.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        L.ref_write_wfx.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
         L.ref_gradient.argtypes = [dp, ctypes.c_int]
         L.ref_gradient.restype = ctypes.c_int
         L.ref_electron_counts.argtypes = [ip, ip]
@@ -116,6 +117,11 @@ def gradient(natom: int) -> np.ndarray:
 def write_molden(path: str, write_virtual: bool = True) -> None:
     """The reference's Molden file of the last scf() call."""
     lib().ref_write_molden(path.encode(), 1 if write_virtual else 0, 1)
+
+
+def write_wfx(path: str, write_virtual: bool = True) -> None:
+    """The reference's WFX file of the last scf() call."""
+    lib().ref_write_wfx(path.encode(), 1 if write_virtual else 0, 1)
 
 
 def electron_counts() -> Tuple[int, int]:

@@ -10,6 +10,8 @@ oracle/build_ref.sh and driven through oracle/ref_harness.cpp:
   * <name>.molden  the reference's Molden files (scf::writeOrbitalsMolden, virtual
                    orbitals included) of water 6-31G* (RHF) and CH2 triplet
                    6-31G* (UHF) after converged solves
+  * <name>.wfx     the reference's WFX files (scf::writeOrbitalsWFX, virtual
+                   orbitals included) of the same two solves
   * <name>_grad.npz the nuclear gradient as the derivative of the reference's own
                    converged total energy: a 4-point central difference (step
                    1e-3 bohr, O(h^4)) over SCFs converged to 1e-12.  (The
@@ -134,6 +136,8 @@ def write_molden_cases() -> None:
         refpy.scf(1e-10)
         refpy.write_molden(os.path.join(HERE, name + ".molden"), True)
         print(f"{name}.molden")
+        refpy.write_wfx(os.path.join(HERE, name + ".wfx"), True)
+        print(f"{name}.wfx")
 
 
 def main() -> None:

@@ -141,3 +141,15 @@ def test_reference_harness_reproduces_golden_energy():
     assert E == pytest.approx(float(d["E"]), abs=1e-12)
     # The reference CPU program's published energy for water / STO-3G.
     assert E == pytest.approx(-74.9629349034878, abs=1e-12)
+
+
+def test_oracle_uhf_restart_from_its_fixed_point():
+    # Started from its own converged Li densities, the unrestricted loop stays.
+    d, mol, sh = load_case("li_631g_uhf")
+    n = int(d["nbf"])
+    eri = oracle.eri_tensor(sh)
+    S, H = shells.unpack(d["S"], n), shells.unpack(d["H"], n)
+    a = (S, H, eri, int(d["n_alpha"]), int(d["n_beta"]), float(d["e_nuc"]))
+    E0, Da, Db, it0 = oracle.scf_uhf(*a, max_iter=2000)
+    E1, Da1, Db1, it1 = oracle.scf_uhf(*a, max_iter=2000, guess=(Da, Db))
+    assert abs(E1 - E0) < 1e-12 and it1 <= 3 < it0
