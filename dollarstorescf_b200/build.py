@@ -65,16 +65,17 @@ def _class_tu(c, coop: bool) -> str:
     lines.append("  const int threads = 128;")
     lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
     lines.append("  if (!blocks) return;")
+    lines.append("  const dim3 grid(blocks, a.split > 1 ? (unsigned)a.split : 1u);")
     for boys, pure, mixed in combos:
         pb = "true" if pure else "false"
         mb = "true" if mixed else "false"
         lines.append(f"  if (!uhf && boys == {boys} && pure == {pure} && mixed == {mixed}) "
-                     f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}><<<blocks, threads, 0, s>>>(a);")
+                     f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}><<<grid, threads, 0, s>>>(a);")
     # The unrestricted variant: FP64 with the reference-mode Boys function.
     for pure in (1, 0):
         pb = "true" if pure else "false"
         lines.append(f"  if (uhf && pure == {pure}) "
-                     f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, true><<<blocks, threads, 0, s>>>(a);")
+                     f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, true><<<grid, threads, 0, s>>>(a);")
     lines.append("}")
     if (la, lb) == (lc, ld):
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s) {{")

@@ -666,6 +666,20 @@ int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
     else
       ct.variant = dss_has_coop(ci.la, ci.lb, ci.lc, ci.ld) ? 1 : 0;
     ct.ntasks = (int)ht.tasks[idx].size();
+    // A single molecule whose class has few warp tasks (a small molecule) would
+    // leave most SMs idle while each lane walks its quartet's whole primitive
+    // product, so the thread-per-quartet launch is split into slices of the bra
+    // primitive pairs until the class has about kSplitWarps warps, at most 32
+    // slices and no more than the longest bra contraction.  Batches and large
+    // molecules keep one slice.
+    constexpr long long kSplitWarps = 4736;  // 148 SMs x 32 warps
+    if (ctx->nmol == 0 && ct.ntasks > 0 && ct.ntasks < kSplitWarps) {
+      int max_npp = 1;
+      for (const int4& t : ht.tasks[idx])
+        if ((size_t)t.x < ctx->h_pair_npp.size()) max_npp = std::max(max_npp, ctx->h_pair_npp[t.x]);
+      const long long want = (kSplitWarps + ct.ntasks - 1) / ct.ntasks;
+      ct.split = (int)std::min<long long>(std::min<long long>(want, 32), max_npp);
+    }
     ct.shell_quartets = ht.shell_quartets[idx];
     ct.prim_quartets = ht.prim_quartets[idx];
     ctx->n_warp_tasks += ct.ntasks;
@@ -735,6 +749,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     }
     a.tasks = ct.d_tasks.ptr;
     a.ntasks = ct.ntasks;
+    a.split = ct.split;
     a.pair_a = ctx->d_pair_a.ptr;
     a.pair_b = ctx->d_pair_b.ptr;
     a.pair_pp0 = ctx->d_pair_pp0.ptr;

@@ -72,6 +72,7 @@ struct ClassTasks {
   int la = 0, lb = 0, lc = 0, ld = 0;
   int ntasks = 0;
   int variant = 0;  // 0: thread per quartet, 1: warp-cooperative
+  int split = 1;    // thread-per-quartet launches: slices of the bra primitive pairs
   long long shell_quartets = 0, prim_quartets = 0;
   DevBuf<int4> d_tasks;
 };

@@ -23,8 +23,10 @@
 #include "eri_gen.cuh"
 
 struct EriArgs {
-  const int4* tasks;      // {bra pair, first ket pair, ket count, 0}
+  const int4* tasks;      // {bra pair, first ket pair, ket count, molecule}
   int ntasks;
+  int split;              // thread-per-quartet kernel: blockIdx.y of split slices
+                          // evaluates its share of the bra primitive pairs
   const int* pair_a;      // shell index of a (pair order: l_a >= l_b)
   const int* pair_b;
   const int* pair_pp0;    // first primitive pair
@@ -229,6 +231,16 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
   bool active = lane < t.z;
   const int bra = t.x;
   const int ket = t.y + (active ? lane : 0);
+  // Bra primitive pairs of this slice: all of them, or with split > 1 the
+  // blockIdx.y-th of split equal parts.  The digest is linear in the integrals,
+  // so every slice digests its partial sum and J/K add up to the full quartet.
+  int bpp0 = __ldg(a.pair_pp0 + bra), bnpp = __ldg(a.pair_npp + bra);
+  if (a.split > 1) {
+    const int lo = bnpp * (int)blockIdx.y / a.split, hi = bnpp * ((int)blockIdx.y + 1) / a.split;
+    if (lo == hi) return;  // uniform per warp
+    bpp0 += lo;
+    bnpp = hi - lo;
+  }
   const int sa = __ldg(a.pair_a + bra), sb = __ldg(a.pair_b + bra);
   const int sc = __ldg(a.pair_a + ket), sd = __ldg(a.pair_b + ket);
   const double* __restrict__ Dm = a.D;
@@ -259,7 +271,7 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
     if (active && fp32) {
       float If[NA * NB * NC * ND];
       EriClass<LA, LB, LC, LD>::template evalr<BOYS, PURE, float>(
-          a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
+          a.pp + bpp0, bnpp, a.pp + __ldg(a.pair_pp0 + ket),
           __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, If, a.boys_cell);
 #pragma unroll
       for (int q = 0; q < NA * NB * NC * ND; ++q) I[q] = (double)If[q];
@@ -269,7 +281,7 @@ __global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk
   if (done) {
   } else if (active) {
     EriClass<LA, LB, LC, LD>::template eval<BOYS, PURE>(
-        a.pp + __ldg(a.pair_pp0 + bra), __ldg(a.pair_npp + bra), a.pp + __ldg(a.pair_pp0 + ket),
+        a.pp + bpp0, bnpp, a.pp + __ldg(a.pair_pp0 + ket),
         __ldg(a.pair_npp + ket), Ax - Bx, Ay - By, Az - Bz, Cx - Dx, Cy - Dy, Cz - Dz, I, a.boys_cell);
   } else {
 #pragma unroll

@@ -107,18 +107,11 @@ int dss_write_molden(dss_ctx* ctx, const char* path, int natom, const int* Z, co
   for (int a = 0; a < natom; ++a)
     if (Z[a] < 1 || Z[a] > (int)(sizeof(kSymbols) / sizeof(kSymbols[0])))
       return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_write_molden: element without a symbol here");
-  // Shells of each atom: those centred on it, in basis order.
-  std::vector<std::vector<int>> atom_shells(natom);
-  for (int s = 0; s < ns; ++s) {
+  for (int s = 0; s < ns; ++s)
     if (B.l[s] > 2) return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_write_molden: l above 2");
-    int owner = -1;
-    for (int a = 0; a < natom && owner < 0; ++a)
-      if (B.xyz[3 * s] == xyz_bohr[3 * a] && B.xyz[3 * s + 1] == xyz_bohr[3 * a + 1] &&
-          B.xyz[3 * s + 2] == xyz_bohr[3 * a + 2])
-        owner = a;
-    if (owner < 0) return dss_fail(ctx, DSS_ERR_INVALID, "dss_write_molden: a shell centre is not on any nucleus");
-    atom_shells[owner].push_back(s);
-  }
+  std::vector<std::vector<int>> atom_shells;
+  if (!shells_by_atom(B, natom, xyz_bohr, &atom_shells))
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_write_molden: a shell centre is not on any nucleus");
   FILE* f = std::fopen(path, "wb");
   if (!f) return dss_fail(ctx, DSS_ERR_INVALID, std::string("dss_write_molden: cannot open ") + path);
   std::fprintf(f, "[Molden Format]\n[5D]\n[9G]\n[Atoms] AU\n");
