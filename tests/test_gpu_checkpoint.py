@@ -1,7 +1,8 @@
 """Density checkpoint round trip after device solves: save the converged
 densities, read them back, restart the solve from them.  The restarted solve
 lands on the same energy (1e-9 Eh, the plain form's bar) within a few
-iterations instead of the core guess's dozens, where the saved state is a fixed
+iterations (at most 5: the last ones move with the rounding of the J/K
+atomics) instead of the core guess's dozens, where the saved state is a fixed
 point of the loop; where it is not (the reference's loop stops on |dE| alone),
 the restart follows the reference's loop (the oracle) from the same densities."""
 import numpy as np
@@ -35,7 +36,7 @@ def test_rhf_restart_from_checkpoint(fb, tmp_path):
     E1, D1, it1, rc = fb.scf(d["H"], d["S"], ne, float(d["e_nuc"]), conv=1e-10, guess=Da)
     assert rc == 0
     assert abs(E1 - E0) < 1e-9 and abs(E1 - float(d["E"])) < 1e-9
-    assert it1 <= 3 < it0, (it1, it0)
+    assert it1 <= 5 < it0, (it1, it0)
 
 
 def test_uhf_restart_from_checkpoint(fb, tmp_path):
@@ -54,7 +55,7 @@ def test_uhf_restart_from_checkpoint(fb, tmp_path):
     E1, Da1, Db1, it1, rc = fb.uhf(d["H"], d["S"], na, nb, float(d["e_nuc"]), conv=1e-10, guess=(Da, Db))
     assert rc == 0
     assert abs(E1 - E0) < 1e-9 and abs(E1 - float(d["E"])) < 1e-9
-    assert it1 <= 3 < it0, (it1, it0)
+    assert it1 <= 5 < it0, (it1, it0)
 
 
 def test_uhf_restart_follows_the_reference_loop(fb, tmp_path):
