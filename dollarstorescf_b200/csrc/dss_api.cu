@@ -670,15 +670,22 @@ int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
     // leave most SMs idle while each lane walks its quartet's whole primitive
     // product, so the thread-per-quartet launch is split into slices of the bra
     // primitive pairs until the class has about kSplitWarps warps, at most 32
-    // slices and no more than the longest bra contraction.  Batches and large
-    // molecules keep one slice.
+    // slices and no more than the longest bra contraction.  A class whose
+    // longest primitive product is below kSplitMinProduct has short lanes
+    // already and would only pay each slice's digest atomics.  Batches and
+    // large molecules keep one slice.
     constexpr long long kSplitWarps = 4736;  // 148 SMs x 32 warps
+    constexpr long long kSplitMinProduct = 64;
     if (ctx->nmol == 0 && ct.ntasks > 0 && ct.ntasks < kSplitWarps) {
       int max_npp = 1;
+      long long longest = 1;
       for (const int4& t : ht.tasks[idx])
-        if ((size_t)t.x < ctx->h_pair_npp.size()) max_npp = std::max(max_npp, ctx->h_pair_npp[t.x]);
+        if ((size_t)t.x < ctx->h_pair_npp.size() && (size_t)t.y < ctx->h_pair_npp.size()) {
+          max_npp = std::max(max_npp, ctx->h_pair_npp[t.x]);
+          longest = std::max(longest, (long long)ctx->h_pair_npp[t.x] * ctx->h_pair_npp[t.y]);
+        }
       const long long want = (kSplitWarps + ct.ntasks - 1) / ct.ntasks;
-      ct.split = (int)std::min<long long>(std::min<long long>(want, 32), max_npp);
+      if (longest >= kSplitMinProduct) ct.split = (int)std::min<long long>(std::min<long long>(want, 32), max_npp);
     }
     ct.shell_quartets = ht.shell_quartets[idx];
     ct.prim_quartets = ht.prim_quartets[idx];
