@@ -58,7 +58,7 @@ def _class_tu(c, coop: bool) -> str:
     (two-density) form with the reference Boys function."""
     la, lb, lc, ld = c
     name = f"{la}{lb}{lc}{ld}"
-    lines = [f'#include "{"coop_kernels.cuh" if coop else "eri_kernels.cuh"}"', ""]
+    lines = [f'#include "{"coop_kernels.cuh" if coop else "eri_kernels.cuh"}"', "#include <atomic>", ""]
     combos = [(0, 1, 0), (0, 0, 0), (1, 1, 0), (1, 0, 0), (1, 1, 1), (1, 0, 1)]
     lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, int uhf, const EriArgs& a, "
                  f"cudaStream_t s) {{")
@@ -76,6 +76,20 @@ def _class_tu(c, coop: bool) -> str:
         pb = "true" if pure else "false"
         lines.append(f"  if (uhf && pure == {pure}) "
                      f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, true><<<grid, threads, 0, s>>>(a);")
+    lines.append("}")
+    # Loads (under lazy module loading) the FP64 kernel a plain build of this
+    # class launches, so that the first build allocates no code memory.
+    lines.append(f"void dss_preload_eri_jk_{name}(int boys, int pure, int variant) {{")
+    lines.append("  cudaFuncAttributes fa;")
+    for boys in (0, 1):
+        for pure in (1, 0):
+            pb = "true" if pure else "false"
+            if coop:
+                lines.append(f"  if (variant == 1 && boys == {boys} && pure == {pure}) "
+                             f"{{ cudaFuncGetAttributes(&fa, eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, false>); "
+                             f"return; }}")
+            lines.append(f"  if (boys == {boys} && pure == {pure}) "
+                         f"cudaFuncGetAttributes(&fa, eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, false>);")
     lines.append("}")
     if (la, lb) == (lc, ld):
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s) {{")
@@ -100,13 +114,15 @@ def _class_tu(c, coop: bool) -> str:
             k = f"eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}>"
             sm = f"coop_smem_per_warp<{la}, {lb}, {lc}, {ld}, {pb}>() * sizeof(double) * DSS_COOP_WARPS"
             lines.append(f"  if (boys == {boys} && pure == {pure} && mixed == {mixed}) {{")
-            lines.append(f"    static bool attr[64] = {{}};  // per device: the attribute is per context")
+            lines.append(f"    // per device (the attribute is per context); contexts on several host")
+            lines.append(f"    // threads may race here, and setting the attribute twice is harmless")
+            lines.append(f"    static std::atomic<bool> attr[64] = {{}};")
             lines.append(f"    int dev = 0;")
             lines.append(f"    cudaGetDevice(&dev);")
             lines.append(f"    const size_t smem = {sm};")
-            lines.append(f"    if (dev < 0 || dev >= 64 || !attr[dev]) {{ cudaFuncSetAttribute({k}, "
+            lines.append(f"    if (dev < 0 || dev >= 64 || !attr[dev].load()) {{ cudaFuncSetAttribute({k}, "
                          f"cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); "
-                         f"if (dev >= 0 && dev < 64) attr[dev] = true; }}")
+                         f"if (dev >= 0 && dev < 64) attr[dev].store(true); }}")
             lines.append(f"    {k}<<<blocks, 32 * DSS_COOP_WARPS, smem, s>>>(a);")
             lines.append("  }")
         lines.append("}")
@@ -129,6 +145,13 @@ def _dispatch_tu(classes, pcls, coop) -> str:
         lines.append(f"  if (!uhf && variant == 1 && la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
                      f"return dss_launch_eri_coop_{la}{lb}{lc}{ld}(boys, pure, mixed, a, s);")
     lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, mixed, uhf, a, s);")
+    lines.append("}")
+    for (la, lb, lc, ld) in classes:
+        lines.append(f"void dss_preload_eri_jk_{la}{lb}{lc}{ld}(int boys, int pure, int variant);")
+    lines.append("void dss_preload_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant) {")
+    for (la, lb, lc, ld) in classes:
+        lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
+                     f"return dss_preload_eri_jk_{la}{lb}{lc}{ld}(boys, pure, variant);")
     lines.append("}")
     for (la, lb) in pcls:
         lines.append(f"void dss_launch_schwarz_{la}{lb}(int boys, int pure, const SchwarzArgs& a, cudaStream_t s);")

@@ -17,6 +17,7 @@
 // every molecule whatever its stage.  The eigensolver is the cyclic Jacobi
 // method with one thread block per molecule, the matrix held in shared memory
 // when it fits, warm-started from the previous iteration's vectors.
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -827,18 +828,19 @@ bool same_opts(const dss_scf_opts& a, const dss_scf_opts& c) {
 void launch_jacobi(dss_batch* b, const BatchView& v, int ka, int kv, int kt, int max_sweeps) {
   cudaStream_t s = b->ctx->stream;
   const int nb = (int)b->slot_mol.size();
-  // Shared-memory opt-in per device (the function attribute is per context).
-  static int optin_dev[64] = {};
+  // Shared-memory opt-in per device (the function attribute is per context);
+  // batches on several host threads may both set it, which is harmless.
+  static std::atomic<int> optin_dev[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   int optin = 0;
-  if (dev >= 0 && dev < 64 && optin_dev[dev]) {
-    optin = optin_dev[dev];
+  if (dev >= 0 && dev < 64 && optin_dev[dev].load()) {
+    optin = optin_dev[dev].load();
   } else {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncSetAttribute(k_jacobi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     cudaFuncSetAttribute(k_jacobi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    if (dev >= 0 && dev < 64) optin_dev[dev] = optin;
+    if (dev >= 0 && dev < 64) optin_dev[dev].store(optin);
   }
   auto fits = [&](int nn_, bool vt) {
     return (dss_packed_size(nn_) + (vt ? (size_t)nn_ * nn_ : 0)) * 8 + dss_block_jacobi_smem(nn_) <= (size_t)optin;

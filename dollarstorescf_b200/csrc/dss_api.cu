@@ -198,6 +198,7 @@ int dss_create(dss_ctx** out, const dss_opts* opts) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev[i], cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = dss_noalloc_attach(&ctx->noalloc_acc);
   ctx->stream = ctx->own_stream;
   if (e != cudaSuccess) {
     g_create_error = std::string("dss_create: ") + cudaGetErrorString(e);
@@ -252,6 +253,7 @@ int dss_set_basis(dss_ctx* ctx, int n_shell, const int* l, const int* nprim, con
   ctx->basis = B;
   int rc = dss_setup_pairs(ctx, std::move(B));
   if (rc != DSS_OK) return rc;
+  dss_preload_build(ctx);
   return DSS_OK;
 }
 
@@ -892,10 +894,15 @@ int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
   if (variant == 1 && !dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]))
     return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: no warp-cooperative kernel for this class");
   ctx->class_variant[i] = variant;
-  if ((size_t)i < ctx->tasks.size())
-    ctx->tasks[i].variant = variant >= 0 ? variant : (dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]) ? 1 : 0);
+  if ((size_t)i < ctx->tasks.size()) {
+    ClassTasks& ct = ctx->tasks[i];
+    ct.variant = variant >= 0 ? variant : (dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]) ? 1 : 0);
+    if (ct.ntasks && ctx->nmol == 0 && cudaSetDevice(ctx->opts.device) == cudaSuccess)
+      dss_preload_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, ct.variant);
+  }
   return DSS_OK;
 }
+
 
 int dss_get_class_variant(const dss_ctx* ctx, int i) {
   if (!ctx || i < 0 || (size_t)i >= ctx->tasks.size()) return -1;
@@ -963,6 +970,12 @@ int dss_probe_fp64_peak(dss_ctx* ctx, double* tflops) {
 }
 
 }  // extern "C"
+
+void dss_preload_build(dss_ctx* ctx) {
+  if (ctx->nmol > 0) return;
+  for (const ClassTasks& ct : ctx->tasks)
+    if (ct.ntasks) dss_preload_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, ct.variant);
+}
 
 // ------------------------------------------------------------------ Boys check
 #include "boys.cuh"

@@ -85,6 +85,7 @@ struct ScfBuffers {
 struct dss_ctx {
   dss_opts opts{};
   const double* boys_cell = nullptr;  // device address of the Boys cell records on opts.device
+  double* noalloc_acc = nullptr;      // device address of the allocation-free build's accumulators
   cudaStream_t stream = nullptr;      // the stream work is enqueued on
   cudaStream_t own_stream = nullptr;  // created with the context
   // Side streams: the class launches of one build fork onto them so that the
@@ -172,6 +173,13 @@ struct dss_ctx {
 };
 
 int dss_fail(dss_ctx* ctx, int code, const std::string& msg);
+// Device address of the allocation-free build's accumulator array on the current
+// device; loads the array and its kernels (dss_create calls it, so that
+// dss_build_jk_device_noalloc itself loads and allocates nothing).
+cudaError_t dss_noalloc_attach(double** acc);
+// Loads the kernels a plain build of the context's basis launches (see
+// dss_preload_eri_variant).
+void dss_preload_build(dss_ctx* ctx);
 // Device address of the reference-mode Boys cell records on the current device
 // (defined once in the generated boys_cell_data.cu).
 cudaError_t dss_boys_cell_table(const double** out);

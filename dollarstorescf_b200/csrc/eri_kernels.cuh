@@ -388,5 +388,8 @@ void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a
 void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, int variant,
                             const EriArgs& a, cudaStream_t s);
 bool dss_has_coop(int la, int lb, int lc, int ld);
+// Loads the FP64 kernel of a plain build of the class (variant as above) if the
+// CUDA runtime loads modules lazily, so that its first launch allocates nothing.
+void dss_preload_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant);
 void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, const EriArgs& a,
                        cudaStream_t s);

@@ -2,6 +2,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "linalg.cuh"
 
 namespace cg = cooperative_groups;
@@ -231,19 +233,26 @@ cudaError_t dss_jacobi_eigh(cudaStream_t s, int n, double* A, double* V, double*
                             double tol, bool v_init) {
   int dev = 0;
   cudaGetDevice(&dev);
-  static int optin[64] = {};
-  if (dev >= 0 && dev < 64 && !optin[dev]) {
-    cudaDeviceGetAttribute(&optin[dev], cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncSetAttribute(jacobi_block_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin[dev]);
-    cudaFuncSetAttribute(jacobi_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin[dev]);
+  // Per device: the shared-memory opt-in and the kernels' attribute (set per
+  // context).  Contexts on several host threads may both set it, which is harmless.
+  static std::atomic<int> optin_cache[64] = {};
+  int optin = 0;
+  if (dev >= 0 && dev < 64) {
+    optin = optin_cache[dev].load();
+    if (!optin) {
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      cudaFuncSetAttribute(jacobi_block_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+      cudaFuncSetAttribute(jacobi_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+      optin_cache[dev].store(optin);
+    }
   }
   const size_t one = dss_packed_size(n) * 8 + dss_block_jacobi_smem(n), two = one + (size_t)n * n * 8;
-  if (dev >= 0 && dev < 64 && two <= (size_t)optin[dev]) {
+  if (two <= (size_t)optin) {
     // Small matrices: one block, matrix and rotations in shared memory.
     jacobi_block_kernel<true><<<1, 512, two, s>>>(n, A, V, w, work, max_sweeps, tol, v_init ? 1 : 0);
     return cudaGetLastError();
   }
-  if (dev >= 0 && dev < 64 && one <= (size_t)optin[dev]) {
+  if (one <= (size_t)optin) {
     // Medium: the matrix in shared memory, the rotations in work.
     jacobi_block_kernel<false><<<1, 512, one, s>>>(n, A, V, w, work, max_sweeps, tol, v_init ? 1 : 0);
     return cudaGetLastError();

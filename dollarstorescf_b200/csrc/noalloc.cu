@@ -8,9 +8,13 @@
 // allocator latency.  dss_build_jk_device_noalloc gives them the same build with
 // the accumulators in a fixed array that is part of the loaded library image
 // (every GPU that loads the library holds it until the process exits).
+//
+// With lazy module loading (the CUDA default since 12.2) the array and a
+// kernel's code reach the device on first use, which allocates.  dss_create
+// therefore looks up the array's address here (loading it and the symmetrise
+// kernel), and dss_set_basis loads the class kernels a build launches, so the
+// entry point itself loads and allocates nothing.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "dss.h"
 #include "dss_internal.h"
@@ -20,10 +24,6 @@ namespace {
 // Two n x n accumulators, n <= DSS_NOALLOC_MAX_NBF (4 MiB).
 static __device__ __align__(256) double g_noalloc_acc[2 * DSS_NOALLOC_MAX_NBF * DSS_NOALLOC_MAX_NBF];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double* g_acc_dev[kMaxDevices] = {};  // device address of g_noalloc_acc per device
-
 __global__ void noalloc_symmetrize(const double* __restrict__ acc, double* __restrict__ out, int n) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n * n) return;
@@ -32,6 +32,21 @@ __global__ void noalloc_symmetrize(const double* __restrict__ acc, double* __res
 }
 
 }  // namespace
+
+// Set-up with the context's device current (called by dss_create): the array's
+// name is a host-side stand-in, the kernels need its device address.  The
+// address is kept per context, so a context made after a device reset looks it
+// up again.
+cudaError_t dss_noalloc_attach(double** acc) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_acc);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes fa;
+  e = cudaFuncGetAttributes(&fa, noalloc_symmetrize);
+  if (e != cudaSuccess) return e;
+  *acc = static_cast<double*>(p);
+  return cudaSuccess;
+}
 
 extern "C" int dss_build_jk_device_noalloc(dss_ctx* ctx, const double* D, double* J, double* K) {
   if (!ctx) return DSS_ERR_INVALID;
@@ -44,26 +59,12 @@ extern "C" int dss_build_jk_device_noalloc(dss_ctx* ctx, const double* D, double
     return dss_fail(ctx, DSS_ERR_INVALID,
                     "dss_build_jk_device_noalloc: " + std::to_string(n) + " basis functions exceed the maximum of " +
                         std::to_string(DSS_NOALLOC_MAX_NBF) + " for the built-in accumulators");
-  const int dev = ctx->opts.device;
-  if (dev < 0 || dev >= kMaxDevices) return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk_device_noalloc: device");
-  cudaError_t e = cudaSetDevice(dev);
+  if (!ctx->noalloc_acc)
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_build_jk_device_noalloc: accumulator array not attached");
+  cudaError_t e = cudaSetDevice(ctx->opts.device);
   if (e != cudaSuccess) return dss_cuda_check(ctx, e, "dss_build_jk_device_noalloc: cudaSetDevice");
-  double* acc = nullptr;
-  {
-    // Set-up, once per device with that device current: the array's name is a
-    // host-side stand-in, the kernels need its device address.
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_acc_dev[dev]) {
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_acc);
-      if (e != cudaSuccess)
-        return dss_cuda_check(ctx, e, "dss_build_jk_device_noalloc: cudaGetSymbolAddress");
-      g_acc_dev[dev] = static_cast<double*>(p);
-    }
-    acc = g_acc_dev[dev];
-  }
-  double* Jacc = acc;
-  double* Kacc = acc + (size_t)n * n;
+  double* Jacc = ctx->noalloc_acc;
+  double* Kacc = ctx->noalloc_acc + (size_t)n * n;
   // dss_enqueue_jk zeroes both accumulators before the ERI launches, so nothing
   // left from an earlier call reaches the result.
   int rc = dss_enqueue_jk(ctx, D, Jacc, Kacc);

@@ -7,7 +7,9 @@ every request that has arrived into the running batch while the batch arena has
 room (admission by device memory), runs SCF iterations of all admitted
 molecules together (dss_batch_step: one captured graph per iteration), and
 retires molecules as they finish, so new requests join while others are on the
-GPU.  Per request it records the latency from arrival to result.
+GPU.  Per request it records the latency from arrival to result, split into
+the queue time (arrival to admission) and the service time (admission to
+result); solves/s counts converged results only.
 """
 from __future__ import annotations
 
@@ -48,6 +50,16 @@ class Result:
     @property
     def latency(self) -> float:
         return self.finished - self.arrival
+
+    @property
+    def queue(self) -> float:
+        """Arrival to admission: time spent waiting for a slot (arena memory)."""
+        return self.admitted - self.arrival
+
+    @property
+    def service(self) -> float:
+        """Admission to result: time on the GPU, shared with the other molecules."""
+        return self.finished - self.admitted
 
 
 def poisson_arrivals(rate: float, count: int, seed: int) -> np.ndarray:
@@ -146,14 +158,26 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
         if own:
             b.close()
     wall = time.perf_counter() - t0
-    lat = np.array([r.latency for r in results])
+
+    def pct(vals, q):
+        return float(np.percentile(np.array(vals), q) * 1e3) if len(vals) else None
+
+    lat = [r.latency for r in results]
+    que = [r.queue for r in results]
+    svc = [r.service for r in results]
+    ok = sum(1 for r in results if r.status == 0)
     return {
         "results": results,
         "solves": len(results),
+        "converged": ok,
         "wall_s": wall,
-        "solves_per_s": len(results) / wall if wall > 0 else 0.0,
-        "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
-        "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
+        "solves_per_s": ok / wall if wall > 0 else 0.0,
+        "p50_ms": pct(lat, 50),
+        "p99_ms": pct(lat, 99),
+        "queue_p50_ms": pct(que, 50),
+        "queue_p99_ms": pct(que, 99),
+        "service_p50_ms": pct(svc, 50),
+        "service_p99_ms": pct(svc, 99),
         "peak_inflight": peak_inflight,
         "admissions_deferred": admissions_deferred,
     }

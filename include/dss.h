@@ -100,13 +100,15 @@ int dss_build_jk_mixed_device(dss_ctx* ctx, const double* D_dense_dev, double* J
  * a pool or budget, latency-bound loops.  The two n x n accumulators live in a
  * fixed 4 MiB array inside the library (held on every GPU that loads the
  * library until the process exits), so n may not exceed DSS_NOALLOC_MAX_NBF;
- * larger bases are rejected with DSS_ERR_INVALID.  The first call on a device
- * looks up the array's device address; make that first call before any stream
- * capture.  The array is zeroed at the start of every call and keeps the last
- * call's accumulators afterwards; every call on a device shares it, so calls
- * whose GPU work overlaps (other streams or contexts on the same device) race.
- * Inputs, outputs and the basis context are the caller's, as for
- * dss_build_jk_device; single-molecule contexts only. */
+ * larger bases are rejected with DSS_ERR_INVALID.  dss_create looks up the
+ * array's device address (with lazy module loading this is when the array
+ * reaches the device), and dss_set_basis / dss_set_class_variant load the
+ * kernels a build launches, so the call itself loads and allocates nothing,
+ * its first call included.  The array is zeroed at the start of every call and
+ * keeps the last call's accumulators afterwards; every call on a device shares
+ * it, so calls whose GPU work overlaps (other streams or contexts on the same
+ * device) race.  Inputs, outputs and the basis context are the caller's, as
+ * for dss_build_jk_device; single-molecule contexts only. */
 int dss_build_jk_device_noalloc(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev);
 
 /* Waits for the context's stream. */

@@ -16,6 +16,10 @@
 //                         chem/scf/ExactCoulomb.cpp:41-72
 //   single ERI            flo::electronRepulsionIntegral chem/GaussianIntegral.cpp:561-642
 //   Boys                  flo::boysFunctionExact     chem/GaussianIntegral.cpp:209-223
+#include <sys/mman.h>
+#include <sys/wait.h>
+#include <unistd.h>
+
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -30,6 +34,7 @@
 #include "chem/scf/ExactCoulomb.hpp"
 #include "chem/scf/SCFBasis.hpp"
 #include "chem/scf/SCFCommon.hpp"
+#include "chem/scf/SCFDIIS.hpp"
 #include "chem/scf/SCFSolver.hpp"
 #include "chem/scf/WriteOrbitals.hpp"
 #include "chem/scf/Gradient.hpp"
@@ -45,6 +50,22 @@ extern uint iteration;
 void assignOverlapMatrix();
 void assignCoreHamiltonian();
 void assignOrthogonalization();
+// Non-static definitions of chem/scf/ExactCoulomb.cpp:13-15, SCFSolver.cpp and
+// Energy.cpp:13-18 that the parallel drivers below reuse.  The tensor globals
+// are weak references: the drop-in variant of this library replaces
+// ExactCoulomb.cpp with the GPU shim and has no stored tensor (the parallel
+// fill then reports failure instead of running).
+extern std::vector<double> repulsion_tensor __attribute__((weak));
+extern size_t diagonal_size __attribute__((weak));
+extern size_t tensor_size __attribute__((weak));
+extern double previous_electronic_energy;
+extern double total_electronic_energy;
+extern double kinetic_energy, nuclear_attraction_energy, electron_repulsion_energy, exchange_energy,
+    correlation_energy, nuclear_energy;
+void updateFockMatrix(Spin spin);
+void solveRoothaanHall(Spin spin);
+void computeDensityMatrix(const Spin spin);
+bool checkConvergence();
 }  // namespace scf
 
 namespace {
@@ -127,6 +148,139 @@ void load_packed(flo::SymmetricMatrixNd& m, const double* in) {
   for (size_t x = 0; x < n; ++x)
     for (size_t y = 0; y <= x; ++y) m.at((uint)y, (uint)x) = in[x * (x + 1) / 2 + y];
 }
+
+// ---------------------------------------------------------------- parallel drivers
+// The reference is single-threaded with global state (chem/GaussianIntegral.cpp:10,
+// chem/scf/SCFCommon.hpp), so threads are ruled out.  For bases whose serial run
+// takes hours ((H2O)16 in 6-31G*), the drivers below fork worker processes that
+// call the same reference functions on disjoint items and return results through
+// shared anonymous mappings; the parent then stores them exactly where the
+// reference's own loops would.  Every value is the reference's own, computed by
+// the same function with the same arguments, so the results are bitwise those of
+// the serial loops.
+int g_workers = 1;
+
+void* shared_alloc(size_t bytes) {
+  void* p = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+  return p == MAP_FAILED ? nullptr : p;
+}
+
+// body(item) for item in [0, count), items pulled from a shared counter by
+// g_workers forked processes.  Returns 0 when every worker exited cleanly.
+template <class F>
+int fork_for(long long count, F body) {
+  long long* ctr = static_cast<long long*>(shared_alloc(4096));
+  if (!ctr) return -1;
+  *ctr = 0;
+  std::cout.flush();
+  std::cerr.flush();
+  std::vector<pid_t> kids;
+  int rc = 0;
+  for (int w = 0; w < g_workers; ++w) {
+    pid_t p = fork();
+    if (p == 0) {
+      for (;;) {
+        long long it = __atomic_fetch_add(ctr, 1LL, __ATOMIC_RELAXED);
+        if (it >= count) break;
+        body(it);
+      }
+      _exit(0);
+    }
+    if (p < 0) {
+      rc = -1;
+      break;
+    }
+    kids.push_back(p);
+  }
+  for (pid_t p : kids) {
+    int st = 0;
+    if (waitpid(p, &st, 0) < 0 || !WIFEXITED(st) || WEXITSTATUS(st) != 0) rc = -1;
+  }
+  munmap(ctr, 4096);
+  return rc;
+}
+
+void decode_pair(size_t m, uint& i, uint& j) {
+  i = (uint)((std::sqrt(8.0 * (double)m + 1.0) - 1.0) / 2.0);
+  while ((size_t)i * (i + 1) / 2 > m) --i;
+  while ((size_t)(i + 1) * (i + 2) / 2 <= m) ++i;
+  j = (uint)(m - (size_t)i * (i + 1) / 2);
+}
+
+// assignExactRepulsionTensor (chem/scf/ExactCoulomb.cpp:41-72) over workers: the
+// same diagonal screen, index formula and electronRepulsionIntegral arguments;
+// one item is one bra pair m = pair(i, j) with every ket pair n >= m.
+int fill_tensor_parallel() {
+  using namespace scf;
+  if (!&repulsion_tensor || !&diagonal_size || !&tensor_size) return -1;
+  const uint nb = (uint)basis.size();
+  flo::SymmetricMatrixNd diagonal_terms(nb);
+  for (uint a = 0; a < nb; ++a)
+    for (uint b = 0; b <= a; ++b)
+      diagonal_terms.at(b, a) = flo::electronRepulsionIntegral(basis[a], basis[b], basis[a], basis[b]);
+  diagonal_size = (size_t)nb * (nb + 1) / 2;
+  tensor_size = diagonal_size * (diagonal_size + 1) / 2;
+  double* sh = static_cast<double*>(shared_alloc(tensor_size * sizeof(double)));
+  if (!sh) return -1;
+  const double thr = 0.00000001 * 0.00000001;  // INTEGRAL_THRESHOLD^2 (ExactCoulomb.cpp:11,63)
+  int rc = fork_for((long long)diagonal_size, [&](long long item) {
+    const size_t m = (size_t)item;
+    uint i, j;
+    decode_pair(m, i, j);
+    for (size_t n = m; n < diagonal_size; ++n) {
+      uint k, l;
+      decode_pair(n, k, l);
+      const size_t index = tensor_size - (diagonal_size - m) * (diagonal_size - m + 1) / 2 + n - m;
+      if (diagonal_terms(i, j) * diagonal_terms(k, l) > thr)
+        sh[index] = flo::electronRepulsionIntegral(basis[i], basis[k], basis[j], basis[l]);
+    }
+  });
+  if (rc == 0) {
+    repulsion_tensor.clear();
+    repulsion_tensor.shrink_to_fit();
+    repulsion_tensor.assign(sh, sh + tensor_size);
+  }
+  munmap(sh, tensor_size * sizeof(double));
+  return rc;
+}
+
+// computeCoulombTerms(spin) followed by computeExchangeTerms(spin)
+// (SCFSolver.cpp:29-43): G(mu,nu) = getExactCoulombMatrix(mu,nu), then
+// -= getExactExchangeMatrix(mu,nu,spin).  With workers, rows mu are spread over
+// processes and the parent performs the same two stores.
+int two_electron_terms(scf::Spin spin, bool coulomb, bool exchange) {
+  using namespace scf;
+  const uint n = matrix_size;
+  if (g_workers <= 1) {
+    if (coulomb) computeCoulombTerms(spin);
+    if (exchange) computeExchangeTerms(spin);
+    return 0;
+  }
+  const size_t P = (size_t)n * (n + 1) / 2;
+  double* sh = static_cast<double*>(shared_alloc(2 * P * sizeof(double)));
+  if (!sh) return -1;
+  double* J = sh;
+  double* K = sh + P;
+  int rc = fork_for((long long)n, [&](long long item) {
+    const uint mu = (uint)item;
+    for (uint nu = mu; nu < n; ++nu) {
+      const size_t idx = (size_t)nu * (nu + 1) / 2 + mu;
+      if (coulomb) J[idx] = getExactCoulombMatrix(mu, nu);
+      if (exchange) K[idx] = getExactExchangeMatrix(mu, nu, spin);
+    }
+  });
+  if (rc == 0) {
+    flo::SymmetricMatrixNd& G = two_electron_hamiltonian[(int)spin];
+    if (coulomb)
+      for (uint mu = 0; mu < n; ++mu)
+        for (uint nu = mu; nu < n; ++nu) G.at(mu, nu) = J[(size_t)nu * (nu + 1) / 2 + mu];
+    if (exchange)
+      for (uint mu = 0; mu < n; ++mu)
+        for (uint nu = mu; nu < n; ++nu) G.at(mu, nu) -= K[(size_t)nu * (nu + 1) / 2 + mu];
+  }
+  munmap(sh, 2 * P * sizeof(double));
+  return rc;
+}
 }  // namespace
 
 extern "C" {
@@ -154,7 +308,10 @@ int ref_setup(int natom, const int* Z, const double* xyz_bohr, int nshell, const
     scf::atom_bases[shell_atom[s]].push_back(flo::GTOShell((uint)shell_l[s], prims));
   }
   g_have_tensor = false;
-  if (!cartesian && build_tensor) {
+  // Parallel tensor fill for closed-shell set-ups only (the unrestricted state
+  // arrays are sized by constructBasis itself).
+  const bool par = g_workers > 1 && multiplicity == 1;
+  if (!cartesian && build_tensor && !par) {
     scf::constructBasis();
     g_have_tensor = true;
   } else {
@@ -177,7 +334,14 @@ int ref_setup(int natom, const int* Z, const double* xyz_bohr, int nshell, const
     }
     size_state_and_one_electron();
     if (build_tensor) {
-      scf::assignExactRepulsionTensor();
+      if (par) {
+        if (fill_tensor_parallel() != 0) {
+          if (quiet) quiet_off();
+          return -1;
+        }
+      } else {
+        scf::assignExactRepulsionTensor();
+      }
       g_have_tensor = true;
     }
   }
@@ -282,12 +446,98 @@ int ref_jk(const double* D_alpha_packed, double* J_packed, double* K_packed) {
   size_t n = scf::basis.size();
   load_packed(scf::density_matrix[0], D_alpha_packed);
   scf::total_density_matrix = 2.0 * scf::density_matrix[0];
+  if (g_workers > 1) {
+    const size_t P = n * (n + 1) / 2;
+    double* sh = static_cast<double*>(shared_alloc(2 * P * sizeof(double)));
+    if (!sh) return -1;
+    int rc = fork_for((long long)n, [&](long long item) {
+      const uint mu = (uint)item;
+      for (uint nu = mu; nu < n; ++nu) {
+        sh[(size_t)nu * (nu + 1) / 2 + mu] = scf::getExactCoulombMatrix(mu, nu);
+        sh[P + (size_t)nu * (nu + 1) / 2 + mu] = scf::getExactExchangeMatrix(mu, nu, scf::Spin::alpha);
+      }
+    });
+    if (rc == 0) {
+      std::memcpy(J_packed, sh, P * sizeof(double));
+      std::memcpy(K_packed, sh + P, P * sizeof(double));
+    }
+    munmap(sh, 2 * P * sizeof(double));
+    return rc;
+  }
   for (uint mu = 0; mu < n; ++mu)
     for (uint nu = mu; nu < n; ++nu) {
       J_packed[(size_t)nu * (nu + 1) / 2 + mu] = scf::getExactCoulombMatrix(mu, nu);
       K_packed[(size_t)nu * (nu + 1) / 2 + mu] = scf::getExactExchangeMatrix(mu, nu, scf::Spin::alpha);
     }
   return 0;
+}
+
+// Worker processes for the drivers above (1: the reference's serial loops).
+// Closed-shell only: ref_setup fills the tensor in parallel for multiplicity 1,
+// and ref_scf_capped runs the restricted iteration.
+void ref_set_workers(int n) { g_workers = n > 1 ? n : 1; }
+
+// scf::useCoreGuess + scf::solveMOs + scf::calculateEnergies for a closed-shell
+// set-up (chem/scf/SCFSolver.cpp:145-237, chem/scf/Energy.cpp:21-50), step by
+// step with the reference's own functions: the same iteration (two-electron
+// terms, updateFockMatrix, solveRoothaanHall, computeDensityMatrix,
+// getTotalElectronicEnergy), the same stop (checkConvergence) and the same final
+// energy terms.  Two differences, both outside the arithmetic: the two-electron
+// terms may be spread over worker processes (ref_set_workers), and the loop
+// stops after max_iter iterations (the reference has no cap; 0 = none), in
+// which case the return value is -(iterations) and E_total is the energy of
+// the last iterate.  Returns the iteration count otherwise.
+int ref_scf_capped(double conv, int max_iter, double* E_total, double* D_alpha_packed, double* seconds,
+                   double* E_trace, int quiet) {
+  using namespace scf;
+  if (!g_have_tensor || spin_treatment != SpinTreatment::restricted) return -1000000;
+  if (quiet) quiet_on();
+  energy_threshold = conv;
+  auto t0 = std::chrono::steady_clock::now();
+  useCoreGuess();
+  iteration = 0;
+  diis::setIterationCount(8);
+  total_electronic_energy = 0.0;
+  previous_electronic_energy = 0.0;
+  bool capped = false;
+  int rc = 0;
+  while (!checkConvergence()) {
+    if (max_iter > 0 && (int)iteration >= max_iter) {
+      capped = true;
+      break;
+    }
+    ++iteration;
+    rc |= two_electron_terms(Spin::alpha, true, true);
+    updateFockMatrix(Spin::alpha);
+    solveRoothaanHall(Spin::alpha);
+    computeDensityMatrix(Spin::alpha);
+    previous_electronic_energy = total_electronic_energy;
+    total_electronic_energy = getTotalElectronicEnergy();
+    if (E_trace && iteration <= 4096) E_trace[iteration - 1] = total_electronic_energy;
+  }
+  // calculateEnergies (Energy.cpp:21-50), restricted branch.
+  kinetic_energy = flo::trace(total_density_matrix * kinetic_energy_matrix);
+  nuclear_attraction_energy = flo::trace(total_density_matrix * nuclear_attraction_matrix);
+  rc |= two_electron_terms(Spin::alpha, true, false);
+  electron_repulsion_energy = 0.5 * flo::trace(density_matrix[0] * two_electron_hamiltonian[0]);
+  electron_repulsion_energy *= 2.0;
+  two_electron_hamiltonian[0] = 0.0;
+  rc |= two_electron_terms(Spin::alpha, false, true);
+  exchange_energy = 0.5 * flo::trace(density_matrix[0] * two_electron_hamiltonian[0]);
+  exchange_energy *= 2.0;
+  correlation_energy = 0.0;
+  nuclear_energy = 0.0;
+  for (int i = 0; i < (int)molecule.size(); ++i)
+    for (int j = i + 1; j < (int)molecule.size(); ++j)
+      nuclear_energy += (int)molecule[i].element * (int)molecule[j].element /
+                        flo::length(molecule[i].position - molecule[j].position);
+  auto t1 = std::chrono::steady_clock::now();
+  *E_total = getTotalEnergy();
+  if (D_alpha_packed) copy_packed(density_matrix[0], D_alpha_packed);
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (quiet) quiet_off();
+  if (rc) return -1000000;
+  return capped ? -(int)iteration : (int)iteration;
 }
 
 // (mu nu | sigma tau) in chemist notation; argument order of the reference is

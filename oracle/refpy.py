@@ -61,6 +61,9 @@ def lib():
         L.ref_time_eri_random.restype = ctypes.c_longlong
         L.ref_time_jk.argtypes = [dp]
         L.ref_time_jk.restype = ctypes.c_double
+        L.ref_set_workers.argtypes = [ctypes.c_int]
+        L.ref_scf_capped.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, ctypes.c_int]
+        L.ref_scf_capped.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -94,6 +97,31 @@ def scf(conv: float = 1e-10) -> Tuple[float, np.ndarray, int, float]:
     if it < 0:
         raise RuntimeError("reference state has no ERI tensor")
     return E.value, D, it, secs.value
+
+
+def set_workers(n: int) -> None:
+    """Worker processes for the closed-shell tensor fill, J/K and SCF drivers
+    (1: the reference's own serial loops).  Results are bitwise the same."""
+    lib().ref_set_workers(int(n))
+
+
+def scf_capped(conv: float = 1e-10, max_iter: int = 0):
+    """Closed-shell SCF through the reference's own iteration functions with an
+    optional iteration cap (0: none, like the reference).  Returns
+    (E_total, D_alpha packed, iterations, converged, seconds, per-iteration
+    electronic energies)."""
+    L = lib()
+    n = L.ref_nbf()
+    E = ctypes.c_double()
+    secs = ctypes.c_double()
+    D = np.zeros(n * (n + 1) // 2)
+    trace = np.zeros(4096)
+    it = L.ref_scf_capped(conv, int(max_iter), ctypes.byref(E), _p(D), ctypes.byref(secs), _p(trace), 1)
+    if it <= -1000000:
+        raise RuntimeError("reference state has no ERI tensor, is open-shell, or a worker failed")
+    conv_ok = it > 0
+    it = abs(it)
+    return E.value, D, it, conv_ok, secs.value, trace[:min(it, 4096)].copy()
 
 
 def spin_density(spin: int) -> np.ndarray:

@@ -22,8 +22,22 @@ oracle/build_ref.sh and driven through oracle/ref_harness.cpp:
                    unrestricted branch): charge, multiplicity, electron counts,
                    the converged energy and both final spin densities, S and H.
 
-Usage (in a container with /root/reference): python tests/golden/make_golden.py [case ...]
-(with case names: only those fixtures; (H2O)8 takes several minutes)
+  * w16_631gs[_6d].npz  the bench workload, (H2O)16 6-31G* (seed 2024; 288
+                   spherical / 304 Cartesian functions): the converged energy and
+                   density, J and K at that density, S and H (no random-density
+                   block: each J/K evaluation of the reference takes minutes here).
+  * c<n>_631g.npz / c<n>_631gs.npz  alkanes drawn by the batching and serving
+                   generators (C4, C7, C10 in 6-31G; C6 in 6-31G*), full fixtures.
+
+Closed-shell SCFs run through oracle.refpy.scf_capped: the reference's own
+iteration functions in the reference's order, with J/K optionally spread over
+worker processes (bitwise the same values as its serial loops).
+
+Usage (in a container with the reference sources; DSS_REFERENCE_ROOT names the
+reference checkout, default /root/reference):
+  python tests/golden/make_golden.py [--workers N] [case ...]
+(with case names: only those fixtures; (H2O)8 takes several minutes, the two
+(H2O)16 cases about an hour each with 6 workers)
 """
 from __future__ import annotations
 
@@ -39,7 +53,10 @@ sys.path.insert(0, ROOT)
 from dollarstorescf_b200 import basis, geometry, shells  # noqa: E402
 from oracle import refpy  # noqa: E402
 
-REF_TEST = "/root/reference/test"
+REF_TEST = os.path.join(os.environ.get("DSS_REFERENCE_ROOT", "/root/reference"), "test")
+
+# Cases too large for a random-density block (see the module docstring).
+LEAN = {"w16_631gs", "w16_631gs_6d"}
 
 
 def cases():
@@ -59,6 +76,22 @@ def cases():
     for name, xyz, bas in (("he_631g", "He.xyz", "6-31G"), ("h2_631g", "hydrogen.xyz", "6-31G"),
                            ("testwater_631gs", "water.xyz", "6-31G*")):
         out.append((name, basis.read_xyz(os.path.join(REF_TEST, xyz)), bas, True))
+    # Appended last so that the seeded random densities of the cases above stay
+    # the same in a full regeneration.
+    out += [
+        # The alkane batch draws n ~ U{1..10} with default_rng(4) and seeds each
+        # molecule with its index: molecules 11, 9 and 5 are C4, C7 and C10.
+        # (Molecules 1, 4, 6, 21, 29, 71 and 90, all C10, do not converge from the
+        # core guess in the reference either: molecule 1 settles into a 3-cycle
+        # of energies, molecule 6 is still creeping after 300 iterations.)
+        ("c4_631g", geometry.alkane(4, 11), "6-31G", True),
+        ("c7_631g", geometry.alkane(7, 9), "6-31G", True),
+        ("c10_631g", geometry.alkane(10, 5), "6-31G", True),
+        # Request 2 of the bench's serving stream (make_request_stream, seed 11).
+        ("c6_631gs", geometry.alkane(6, 139343717), "6-31G*", True),
+        ("w16_631gs", geometry.water_cluster(3, 3, 2, 16, seed=2024), "6-31G*", True),
+        ("w16_631gs_6d", geometry.water_cluster(3, 3, 2, 16, seed=2024), "6-31G*", False),
+    ]
     return out
 
 
@@ -141,7 +174,12 @@ def write_molden_cases() -> None:
 
 
 def main() -> None:
-    only = set(sys.argv[1:])
+    args = sys.argv[1:]
+    if "--workers" in args:
+        k = args.index("--workers")
+        refpy.set_workers(int(args[k + 1]))
+        del args[k:k + 2]
+    only = set(args)
     if "molden" in only:
         write_molden_cases()
         only.discard("molden")
@@ -175,19 +213,30 @@ def main() -> None:
 
 
 def write_case(name, mol, bas, pure, rng) -> None:
+    import time
+
     sh = shells.build_shells(mol, basis.builtin_basis(bas), pure=pure)
+    t0 = time.perf_counter()
     n = refpy.setup(sh)
-    E, D, it, secs = refpy.scf(1e-10)
+    if n < 0:
+        raise RuntimeError(f"{name}: reference set-up failed")
+    t_setup = time.perf_counter() - t0
+    E, D, it, ok, secs, _ = refpy.scf_capped(1e-10, 1000)
+    if not ok:
+        raise RuntimeError(f"{name}: the reference SCF did not converge in 1000 iterations")
     J, K = refpy.jk(D)
-    G = refpy.fock_2e(D)
-    A = rng.standard_normal((n, n)) * 0.1
-    Dr = shells.pack(A + A.T)
-    Jr, Kr = refpy.jk(Dr)
+    extra = {}
+    if name not in LEAN:
+        G = refpy.fock_2e(D)
+        A = rng.standard_normal((n, n)) * 0.1
+        Dr = shells.pack(A + A.T)
+        Jr, Kr = refpy.jk(Dr)
+        extra = dict(G=G, D_rand=Dr, J_rand=Jr, K_rand=Kr)
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"), Z=np.asarray(mol.Z), xyz=np.asarray(mol.xyz), basis=bas,
-        pure=pure, nbf=n, E=E, iterations=it, D=D, J=J, K=K, G=G, D_rand=Dr, J_rand=Jr, K_rand=Kr,
-        S=refpy.overlap(), H=refpy.core_hamiltonian(), e_nuc=mol.nuclear_repulsion())
-    print(f"{name:18s} n={n:4d} E={E:.13f} it={it} ({secs:.2f}s)")
+        pure=pure, nbf=n, E=E, iterations=it, D=D, J=J, K=K, S=refpy.overlap(), H=refpy.core_hamiltonian(),
+        e_nuc=mol.nuclear_repulsion(), **extra)
+    print(f"{name:18s} n={n:4d} E={E:.13f} it={it} (set-up {t_setup:.1f}s, SCF {secs:.1f}s)", flush=True)
 
 
 if __name__ == "__main__":

@@ -69,3 +69,29 @@ def test_served_mixed_form_equals_solo_and_within_one_microhartree():
         E64, _, _, _ = solo_energy(req.shells, req.guess)
         assert abs(res.energy - Em) < 1e-9, (req.kind, res.energy, Em)
         assert abs(res.energy - E64) < 1e-6, (req.kind, res.energy, E64)
+
+
+def test_admission_waits_for_memory_and_results_do_not_change():
+    """A small arena: the requests that do not fit wait until finished molecules
+    free their regions (admissions_deferred > 0), and every result still equals
+    the same molecule solved alone."""
+    from dollarstorescf_b200 import basis, shells
+
+    dimer = geometry.water_dimer(3)
+    E0, D0 = serve.solve_parent(dimer)
+    b631 = basis.builtin_basis("6-31G*")
+    disps = geometry.displacements(dimer, 0.005)
+    reqs = [serve.Request(i, 0.0, shells.build_shells(disps[i], b631, pure=True), "dimer displacement", guess=D0)
+            for i in range(8)]
+    with Batch(schwarz_threshold=1e-12, boys_mode=BOYS_REF, arena_bytes=1_000_000) as b:
+        _, free_bytes, region = b.info(n_for_region=36)
+        fits = free_bytes // region
+        assert 1 <= fits < len(reqs)
+        out = serve.serve(reqs, conv=1e-10, batch=b)
+    assert out["solves"] == len(reqs) and out["converged"] == len(reqs)
+    assert out["admissions_deferred"] > 0
+    assert out["peak_inflight"] <= fits
+    assert out["queue_p99_ms"] > 0.0
+    for req, res in zip(reqs, sorted(out["results"], key=lambda r: r.rid)):
+        E, _, it, st = solo_energy(req.shells, req.guess)
+        assert abs(res.energy - E) < 1e-9, (res.rid, res.energy, E)
