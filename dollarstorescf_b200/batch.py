@@ -69,15 +69,16 @@ class Batch:
                                rebuild_every, final_switch)
 
     def step(self, iterations: int = 1, conv: float = 1e-8, max_iter: int = 128, mixed: bool = False,
-             fp32_threshold: float = 1e-7) -> int:
-        o = self.opts(conv, max_iter=max_iter, mixed=mixed, fp32_threshold=fp32_threshold)
+             fp32_threshold: float = 1e-7, **mixed_opts) -> int:
+        """mixed_opts: skip_threshold, rebuild_every, final_switch of the incremental form."""
+        o = self.opts(conv, max_iter=max_iter, mixed=mixed, fp32_threshold=fp32_threshold, **mixed_opts)
         act = ctypes.c_int()
         self._check(self._L.dss_batch_step(self._h, ctypes.byref(o), iterations, ctypes.byref(act)))
         return act.value
 
     def solve(self, conv: float = 1e-8, max_iter: int = 128, mixed: bool = False,
-              fp32_threshold: float = 1e-7) -> None:
-        o = self.opts(conv, max_iter=max_iter, mixed=mixed, fp32_threshold=fp32_threshold)
+              fp32_threshold: float = 1e-7, **mixed_opts) -> None:
+        o = self.opts(conv, max_iter=max_iter, mixed=mixed, fp32_threshold=fp32_threshold, **mixed_opts)
         self._check(self._L.dss_batch_solve(self._h, ctypes.byref(o)))
 
     def result(self, handle: int, nbf: int = 0, want_density: bool = False) -> Tuple[float, Optional[np.ndarray], int, int]:

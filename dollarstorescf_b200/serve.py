@@ -105,11 +105,12 @@ def solve_parent(dimer, boys_mode: int = BOYS_REF, conv: float = 1e-10):
 
 def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boys_mode: int = BOYS_REF,
           arena_bytes: int = 0, iterations_per_step: int = 1, realtime: bool = True,
-          batch: Optional[Batch] = None, mixed: bool = False) -> Dict:
+          batch: Optional[Batch] = None, mixed: bool = False, **mixed_opts) -> Dict:
     """Runs the request stream; returns per-request results and summary stats.
     realtime=True replays arrivals against the wall clock; False admits each
     request as soon as it is reached in arrival order (a closed loop).
-    mixed=True iterates every molecule in the mixed-precision incremental form."""
+    mixed=True iterates every molecule in the mixed-precision incremental form
+    (mixed_opts: its skip_threshold, rebuild_every, final_switch)."""
     own = batch is None
     b = batch if batch is not None else Batch(schwarz_threshold=1e-12, boys_mode=boys_mode, arena_bytes=arena_bytes)
     pending = sorted(requests, key=lambda r: r.arrival)
@@ -120,6 +121,13 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
     t0 = time.perf_counter()
     peak_inflight = 0
     admissions_deferred = 0
+    # Host wall time of admissions and of steps, the latter split by whether the
+    # batch's composition changed since the previous step (which rebuilds its
+    # work lists before iterating).
+    t_admit = 0.0
+    step_changed: List[float] = []
+    step_same: List[float] = []
+    changed = True
     try:
         while qi < len(pending) or waiting or inflight:
             now = time.perf_counter() - t0
@@ -132,7 +140,10 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
             still = []
             for r in waiting:
                 try:
+                    ta = time.perf_counter()
                     h = b.add(r.shells, guess=r.guess)
+                    t_admit += time.perf_counter() - ta
+                    changed = True
                     inflight[h] = (r, time.perf_counter() - t0)
                 except Exception as e:  # arena full: wait for a slot to free up
                     if getattr(e, "code", None) == -2:
@@ -146,13 +157,17 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
                 if qi < len(pending) and realtime:
                     time.sleep(max(0.0, pending[qi].arrival - (time.perf_counter() - t0)))
                 continue
-            b.step(iterations_per_step, conv=conv, max_iter=max_iter, mixed=mixed)
+            ts = time.perf_counter()
+            b.step(iterations_per_step, conv=conv, max_iter=max_iter, mixed=mixed, **mixed_opts)
+            (step_changed if changed else step_same).append(time.perf_counter() - ts)
+            changed = False
             for h in b.finished_handles():
                 if h not in inflight:
                     continue
                 E, _, it, st = b.result(h)
                 r, adm = inflight.pop(h)
                 b.remove(h)
+                changed = True
                 results.append(Result(r.rid, r.kind, E, it, st, r.arrival, adm, time.perf_counter() - t0))
     finally:
         if own:
@@ -180,4 +195,9 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
         "service_p99_ms": pct(svc, 99),
         "peak_inflight": peak_inflight,
         "admissions_deferred": admissions_deferred,
+        "admission_s": t_admit,
+        "steps_after_change": len(step_changed),
+        "step_after_change_ms": float(np.mean(step_changed) * 1e3) if step_changed else None,
+        "steps_unchanged": len(step_same),
+        "step_unchanged_ms": float(np.mean(step_same) * 1e3) if step_same else None,
     }

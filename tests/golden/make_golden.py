@@ -57,6 +57,10 @@ REF_TEST = os.path.join(os.environ.get("DSS_REFERENCE_ROOT", "/root/reference"),
 
 # Cases too large for a random-density block (see the module docstring).
 LEAN = {"w16_631gs", "w16_631gs_6d"}
+# SCF convergence threshold per case (default 1e-10).  The C10 alkane lands on a
+# slowly converging state from the core guess, where |dE| < 1e-10 leaves the
+# energy uncertain at the 1e-9 Eh level; 1e-12 pins it.
+CONV = {"c10_631g": 1e-12}
 
 
 def cases():
@@ -221,9 +225,11 @@ def write_case(name, mol, bas, pure, rng) -> None:
     if n < 0:
         raise RuntimeError(f"{name}: reference set-up failed")
     t_setup = time.perf_counter() - t0
-    E, D, it, ok, secs, _ = refpy.scf_capped(1e-10, 1000)
+    conv = CONV.get(name, 1e-10)
+    E, D, it, ok, secs, _ = refpy.scf_capped(conv, 1000)
     if not ok:
         raise RuntimeError(f"{name}: the reference SCF did not converge in 1000 iterations")
+    extra_conv = {"conv": conv} if name in CONV else {}
     J, K = refpy.jk(D)
     extra = {}
     if name not in LEAN:
@@ -235,7 +241,7 @@ def write_case(name, mol, bas, pure, rng) -> None:
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"), Z=np.asarray(mol.Z), xyz=np.asarray(mol.xyz), basis=bas,
         pure=pure, nbf=n, E=E, iterations=it, D=D, J=J, K=K, S=refpy.overlap(), H=refpy.core_hamiltonian(),
-        e_nuc=mol.nuclear_repulsion(), **extra)
+        e_nuc=mol.nuclear_repulsion(), **extra, **extra_conv)
     print(f"{name:18s} n={n:4d} E={E:.13f} it={it} (set-up {t_setup:.1f}s, SCF {secs:.1f}s)", flush=True)
 
 
