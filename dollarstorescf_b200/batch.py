@@ -62,8 +62,8 @@ class Batch:
 
     @staticmethod
     def opts(conv: float = 1e-8, diis_size: int = 8, max_iter: int = 128, mixed: bool = False,
-             fp32_threshold: float = 1e-7, skip_threshold: float = 1e-12, rebuild_every: int = 8,
-             final_switch: float = 1e-5):
+             fp32_threshold: float = 1e-7, skip_threshold: float = 1e-12, rebuild_every: int = 16,
+             final_switch: float = 1e-8):
         """SCF options; mixed=True selects the mixed-precision incremental form."""
         return _lib.DssScfOpts(conv, diis_size, max_iter, 0, 1 if mixed else 0, fp32_threshold, skip_threshold,
                                rebuild_every, final_switch)

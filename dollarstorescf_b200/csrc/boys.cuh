@@ -30,6 +30,27 @@
 
 #define DSS_PI_REF 3.14159265358979
 
+// The reference's switch to the asymptotic form, x > 1.1 m + 25, evaluated in
+// double precision as it does (1.1 m rounded, then + 25 rounded): the values for
+// m = 0..12 as exact literals, so that the test costs no arithmetic per call.
+__host__ __device__ constexpr double dss_boys_asym_thr(int m) {
+  switch (m) {
+    case 0: return 0x1.9000000000000p+4;
+    case 1: return 0x1.a19999999999ap+4;
+    case 2: return 0x1.b333333333333p+4;
+    case 3: return 0x1.c4ccccccccccdp+4;
+    case 4: return 0x1.d666666666666p+4;
+    case 5: return 0x1.e800000000000p+4;
+    case 6: return 0x1.f99999999999ap+4;
+    case 7: return 0x1.059999999999ap+5;
+    case 8: return 0x1.0e66666666666p+5;
+    case 9: return 0x1.1733333333333p+5;
+    case 10: return 0x1.2000000000000p+5;
+    case 11: return 0x1.28ccccccccccdp+5;
+    default: return 0x1.319999999999ap+5;
+  }
+}
+
 // 1/(2k+1) for k = 0..255 (g_odd_inv in boys_tab.cuh): the series divides
 // 2x/(2m+2i+1) become products with a correctly rounded reciprocal.
 __device__ __forceinline__ double odd_inv(int k) { return g_odd_inv[k]; }
@@ -65,7 +86,7 @@ static __device__ __noinline__ void boys_ref_series(double x, double* F) {
   int m_series_lo = L + 1;
 #pragma unroll
   for (int m = L; m >= 0; --m) {
-    const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
+    const double thr = dss_boys_asym_thr(m);
     if (!(x > thr)) m_series_lo = m;
   }
   // Top series (m = L) when it is needed.
@@ -183,7 +204,7 @@ __device__ __forceinline__ void boys_ref_walk(double x, double* F) {
   int m_series_lo = L + 1;
 #pragma unroll
   for (int m = L; m >= 0; --m) {
-    const double thr = __dadd_rn(__dmul_rn((double)m, 1.1), 25.0);
+    const double thr = dss_boys_asym_thr(m);
     if (!(x > thr)) m_series_lo = m;
   }
   // The reference's asymptotic form (2m-1)!!/2^(m+1) sqrt(PI/x^(2m+1)) for the low
@@ -226,7 +247,10 @@ __device__ __forceinline__ void boys_ref_walk(double x, double* F) {
     }
   }
   if (use_series) {
-    boys_ref_series<L>(x, F);
+    double Fs[L + 1];
+    boys_ref_series<L>(x, Fs);
+#pragma unroll
+    for (int m = 0; m <= L; ++m) F[m] = Fs[m];
     return;
   }
   // Accurate F_L (7-term Taylor about the nearest table point).
@@ -312,7 +336,7 @@ __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double
   int m_lo = L + 1;
 #pragma unroll
   for (int m = L; m >= 0; --m)
-    if (!(x > __dadd_rn(__dmul_rn((double)m, 1.1), 25.0))) m_lo = m;
+    if (!(x > dss_boys_asym_thr(m))) m_lo = m;
   if (m_lo > 0) {
     // (2m-1)!!/2^(m+1) sqrt(PI) x^-(m+1/2), (2m-1)!! as the reference's 32-bit int.
     const double y = rsqrt(x);
@@ -355,7 +379,14 @@ __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double
     F[m] = f;
     series = series || fabs(x - b) <= 4e-14 * x;
   }
-  if (series) boys_ref_series<L>(x, F);
+  if (series) {
+    // A private array for the (non-inlined) series, so that F itself stays in
+    // registers on the common path.
+    double Fs[L + 1];
+    boys_ref_series<L>(x, Fs);
+#pragma unroll
+    for (int m = 0; m <= L; ++m) F[m] = Fs[m];
+  }
 }
 
 #ifndef DSS_BOYS_CELL_LMAX

@@ -169,7 +169,7 @@ class FockBuilder:
     def scf(self, H: np.ndarray, S: np.ndarray, n_alpha: int, e_nuc: float, conv: float = 1e-8,
             diis_size: int = 8, max_iter: int = 128, guess: Optional[np.ndarray] = None,
             raise_on_noconv: bool = True, mixed: bool = False, fp32_threshold: float = 1e-7,
-            skip_threshold: float = 1e-12, rebuild_every: int = 8, final_switch: float = 1e-5):
+            skip_threshold: float = 1e-12, rebuild_every: int = 16, final_switch: float = 1e-8):
         """Device RHF.  Returns (E_total, D_alpha packed-U, iterations, status).
         mixed=True selects the incremental mixed-precision form."""
         n = self.nbf

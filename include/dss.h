@@ -184,8 +184,8 @@ typedef struct dss_scf_opts {
   int incremental;
   double fp32_threshold; /* default 1e-7 */
   double skip_threshold; /* default 1e-12 */
-  int rebuild_every;     /* default 8 */
-  double final_switch;   /* default 1e-5 Eh */
+  int rebuild_every;     /* default 16 */
+  double final_switch;   /* default 1e-8 Eh */
 } dss_scf_opts;
 
 /* Defaults: conv 1e-8 (chem/scf/SCFSolver.cpp:26), diis_size 8 (:214),
