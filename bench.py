@@ -385,7 +385,8 @@ def run_gpu(args):
     def one_build():
         fb.jk_device(Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
 
-    # Per-class kernel choice (untimed): thread-per-quartet vs warp-cooperative.
+    # Per-class kernel shape (untimed): thread per quartet in three register
+    # tiers or warp-cooperative, the fastest by per-launch events.
     from dollarstorescf_b200 import autotune
 
     variants = autotune.tune(fb, Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
@@ -496,6 +497,9 @@ def run_gpu(args):
         "data": "synthetic (seeded (H2O)16 cluster, 3x3x2 lattice 3.0 A, rotation + 0.2 A jitter)",
         "config": {"workload": WORKLOAD, "nbf": n, "shells": sh.nshell, "boys": "reference series",
                    "warp_cooperative_classes": sorted(k for k, v in variants.items() if v == 1),
+                   # Autotuned kernel shape per class: 0 thread per quartet, 2/3 the
+                   # same with fewer resident blocks (more registers), 1 warp per quartet.
+                   "tuned_shapes": variants,
                    "l2": "flushed between steps (512 MiB write)", "parallelism": f"replicas x{ws}"},
         "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": npk * 8,
                 "d2h_bytes_per_step": 2 * npk * 8},

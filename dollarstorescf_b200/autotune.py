@@ -1,11 +1,21 @@
-"""Per-class kernel autotuner.
+"""Per-class kernel shape autotuner.
 
 For every shell-quartet class with work in the current basis, times each kernel
-variant the library offers (0: one thread per quartet, 1: one warp per quartet
-with shared-memory programs) with per-launch CUDA events (dss_profile_build runs
-the classes one after another on one stream) and keeps the faster one.  The
-choice depends on the class and on the quartet count, so it is redone per basis
-and can be cached by (class, pure, boys mode, quartet-count bucket).
+shape the library offers for it and keeps the fastest:
+
+  0  one thread per shell quartet, the default register budget (resident
+     blocks of 128 threads per SM: 8 / 6 / 4 / 1 for total angular momentum
+     L = 0 / 1..2 / 3..4 / >= 5);
+  2  the same with one fewer resident block (more registers per thread, fewer
+     spills, lower occupancy), L <= 4;
+  3  with about half the resident blocks, L <= 4;
+  1  one warp per shell quartet with shared-memory programs (the heavy classes
+     compiled with it).
+
+Timing is per launch with CUDA events (dss_profile_build / dss_batch_profile
+run the classes one after another on one stream), best of `repeats`.  The best
+shape depends on the class and on its quartet count, so the choice is redone
+per basis and can be cached by (class, pure, boys mode, quartet-count bucket).
 """
 from __future__ import annotations
 
@@ -15,6 +25,9 @@ import os
 from typing import Dict, Optional
 
 from .engine import FockBuilder
+
+# Kernel shapes tried per class (see the module docstring).
+VARIANTS = (0, 2, 3, 1)
 
 
 def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
@@ -30,7 +43,7 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
     keys = [f"{names[i]}|{key_extra}|q{int(math.log2(max(1, infos[i][1])))}" for i in range(nc)]
     todo = [i for i in range(nc) if infos[i][1] > 0 and keys[i] not in cache]
     timings = {}
-    for variant in (0, 1):
+    for variant in VARIANTS:
         ok = []
         for i in todo:
             try:
@@ -64,12 +77,12 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
 
 
 def tune_batch(batch, repeats: int = 2) -> Dict[str, int]:
-    """The same per-class choice for a dss_batch: times both variants of every
+    """The same per-class choice for a dss_batch: times every shape of every
     class with work over all live molecules (dss_batch_profile) and keeps the
-    faster one.  Returns {class name: variant}."""
+    fastest.  Returns {class name: variant}."""
     nc = batch._L.dss_num_classes()
     timings: Dict[int, Dict[int, float]] = {}
-    for variant in (0, 1):
+    for variant in VARIANTS:
         ok = []
         for i in range(nc):
             try:

@@ -60,8 +60,9 @@ def _class_tu(c, coop: bool) -> str:
     name = f"{la}{lb}{lc}{ld}"
     lines = [f'#include "{"coop_kernels.cuh" if coop else "eri_kernels.cuh"}"', "#include <atomic>", ""]
     combos = [(0, 1, 0), (0, 0, 0), (1, 1, 0), (1, 0, 0), (1, 1, 1), (1, 0, 1)]
-    lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, int uhf, const EriArgs& a, "
-                 f"cudaStream_t s) {{")
+    lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, int uhf, int tier, "
+                 f"const EriArgs& a, cudaStream_t s) {{")
+    tiers = la + lb + lc + ld <= 4  # dss_has_tiers
     lines.append("  const int threads = 128;")
     lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
     lines.append("  if (!blocks) return;")
@@ -69,6 +70,12 @@ def _class_tu(c, coop: bool) -> str:
     for boys, pure, mixed in combos:
         pb = "true" if pure else "false"
         mb = "true" if mixed else "false"
+        if tiers and boys == 0 and not mixed:
+            # The plain form: register tier chosen per class by the autotuner.
+            for t in (2, 1):
+                lines.append(f"  if (!uhf && boys == 0 && pure == {pure} && mixed == 0 && tier == {t}) "
+                             f"return eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, false, {t}>"
+                             f"<<<grid, threads, 0, s>>>(a);")
         lines.append(f"  if (!uhf && boys == {boys} && pure == {pure} && mixed == {mixed}) "
                      f"eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}><<<grid, threads, 0, s>>>(a);")
     # The unrestricted variant: FP64 with the reference-mode Boys function.
@@ -88,6 +95,11 @@ def _class_tu(c, coop: bool) -> str:
                 lines.append(f"  if (variant == 1 && boys == {boys} && pure == {pure}) "
                              f"{{ cudaFuncGetAttributes(&fa, eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, false>); "
                              f"return; }}")
+            if tiers and boys == 0:
+                for t in (2, 1):
+                    lines.append(f"  if (variant == {t + 1} && boys == 0 && pure == {pure}) {{ "
+                                 f"cudaFuncGetAttributes(&fa, eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, "
+                                 f"false, {t}>); return; }}")
             lines.append(f"  if (boys == {boys} && pure == {pure}) "
                          f"cudaFuncGetAttributes(&fa, eri_jk_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, false>);")
     lines.append("}")
@@ -144,7 +156,7 @@ def _dispatch_tu(classes, pcls, coop) -> str:
     for (la, lb, lc, ld) in coop:
         lines.append(f"  if (!uhf && variant == 1 && la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
                      f"return dss_launch_eri_coop_{la}{lb}{lc}{ld}(boys, pure, mixed, a, s);")
-    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, mixed, uhf, a, s);")
+    lines.append("  dss_launch_eri_jk(la, lb, lc, ld, boys, pure, mixed, uhf, variant >= 2 ? variant - 1 : 0, a, s);")
     lines.append("}")
     for (la, lb, lc, ld) in classes:
         lines.append(f"void dss_preload_eri_jk_{la}{lb}{lc}{ld}(int boys, int pure, int variant);")
@@ -160,10 +172,10 @@ def _dispatch_tu(classes, pcls, coop) -> str:
         lines.append(f"  if (la == {la} && lb == {lb}) return dss_launch_schwarz_{la}{lb}(boys, pure, a, s);")
     lines.append("}")
     lines.append("void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, "
-                 "const EriArgs& a, cudaStream_t s) {")
+                 "int tier, const EriArgs& a, cudaStream_t s) {")
     for (la, lb, lc, ld) in classes:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
-                     f"return dss_launch_eri_jk_{la}{lb}{lc}{ld}(boys, pure, mixed, uhf, a, s);")
+                     f"return dss_launch_eri_jk_{la}{lb}{lc}{ld}(boys, pure, mixed, uhf, tier, a, s);")
     lines.append("}")
     return "\n".join(lines) + "\n"
 

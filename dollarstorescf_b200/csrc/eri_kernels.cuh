@@ -135,6 +135,18 @@ __device__ __forceinline__ double quartet_dbound(const EriArgs& a, int sa, int s
 // are latency bound and want more warps; the heavy ones keep their registers.
 __host__ __device__ constexpr int dss_min_blocks(int L) { return L == 0 ? 8 : (L <= 2 ? 6 : (L <= 4 ? 4 : 1)); }
 
+// Register tiers of the plain-form thread-per-quartet kernel (the autotuner's
+// shape choice, class variants 0, 2, 3): tier 0 is dss_min_blocks; tiers 1 and 2
+// allow fewer resident 128-thread blocks and so more registers per thread
+// (64/80/128 -> 80/96/168 -> 128/128/255 for L = 0 / 1..2 / 3..4), trading
+// occupancy for fewer spills.  Classes with L >= 5 have one tier.
+__host__ __device__ constexpr int dss_min_blocks_tier(int L, int tier) {
+  return tier == 0 ? dss_min_blocks(L)
+                   : (tier == 1 ? (L == 0 ? 6 : (L <= 2 ? 5 : (L <= 4 ? 3 : 1)))
+                                : (L == 0 ? 4 : (L <= 2 ? 4 : (L <= 4 ? 2 : 1))));
+}
+__host__ __device__ constexpr bool dss_has_tiers(int L) { return L <= 4; }
+
 // The four exchange target blocks of one quartet (Kacc[i][l] += s (ij|kl) D[j][k]
 // and the three others), one block at a time, from density D into Km.
 template <int NA, int NB, int NC, int ND>
@@ -220,8 +232,9 @@ __device__ __forceinline__ void digest_k(const double* I, double s, const double
 
 // UHF = true: the unrestricted variant (one molecule): J from a.D = D_a + D_b,
 // K from a.Da into a.K and from a.Db into a.K2, from one evaluation of the integrals.
-template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false, bool UHF = false>
-__global__ void __launch_bounds__(128, dss_min_blocks(LA + LB + LC + LD)) eri_jk_kernel(EriArgs a) {
+// TIER: register tier (dss_min_blocks_tier).
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false, bool UHF = false, int TIER = 0>
+__global__ void __launch_bounds__(128, dss_min_blocks_tier(LA + LB + LC + LD, TIER)) eri_jk_kernel(EriArgs a) {
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
   constexpr int NC = dss_nfunc(LC, PURE), ND = dss_nfunc(LD, PURE);
   const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -378,18 +391,21 @@ __global__ void __launch_bounds__(128) schwarz_kernel(SchwarzArgs a) {
 
 // Host-side launchers (one translation unit per class defines them).
 #define DSS_DECLARE_LAUNCHERS(la, lb, lc, ld, bc, kc) \
-  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, int mixed, int uhf, const EriArgs& a, cudaStream_t s);
+  void dss_launch_eri_jk_##la##lb##lc##ld(int boys, int pure, int mixed, int uhf, int tier, const EriArgs& a, \
+                                          cudaStream_t s);
 DSS_FOR_EACH_CLASS(DSS_DECLARE_LAUNCHERS)
 #undef DSS_DECLARE_LAUNCHERS
 
 void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s);
-// variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class).
-// uhf = 1: the unrestricted variant (thread per quartet, reference Boys only).
+// variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class);
+// 2, 3: one thread per quartet in register tier 1, 2 (plain form: reference Boys,
+// FP64; other forms run tier 0).  uhf = 1: the unrestricted variant (thread per
+// quartet, reference Boys only).
 void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, int variant,
                             const EriArgs& a, cudaStream_t s);
 bool dss_has_coop(int la, int lb, int lc, int ld);
 // Loads the FP64 kernel of a plain build of the class (variant as above) if the
 // CUDA runtime loads modules lazily, so that its first launch allocates nothing.
 void dss_preload_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant);
-void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, const EriArgs& a,
-                       cudaStream_t s);
+void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, int tier,
+                       const EriArgs& a, cudaStream_t s);

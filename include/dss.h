@@ -135,7 +135,10 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* shell_quartets
 
 /* Kernel variant of class i: 0 one thread per shell quartet, 1 one warp per
  * shell quartet (shared-memory programs; only for the classes compiled with it),
- * -1 the library default.  Used by the autotuner; persists across bases. */
+ * 2 and 3 one thread per shell quartet with one and two fewer resident blocks
+ * per SM and so more registers per thread (classes of total angular momentum
+ * <= 4; the plain FP64 reference-Boys build, other forms run variant 0's
+ * kernel), -1 the library default.  Used by the autotuner; persists across bases. */
 int dss_set_class_variant(dss_ctx* ctx, int i, int variant);
 
 /* The variant class i currently runs with (-1 before a basis is set). */

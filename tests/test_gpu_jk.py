@@ -92,14 +92,15 @@ def test_errors_are_reported_not_fatal(builders):
 
 @pytest.mark.parametrize("name", ["dimer_631gs", "dimer_631gs_6d"])
 def test_kernel_variants_agree(builders, name):
-    # Every class through the thread-per-quartet kernel and, where compiled,
-    # the warp-cooperative one: both must reproduce the reference.
+    # Every class through each kernel shape it has (thread per quartet in the
+    # three register tiers and, where compiled, the warp-cooperative kernel):
+    # all must reproduce the reference.
     d, mol, sh = load_case(name)
     fb = builders[BOYS_REF]
     fb.set_basis(sh)
     n = fb.num_classes()
     results = []
-    for variant in (0, 1):
+    for variant in (0, 2, 3, 1):
         for i in range(n):
             try:
                 fb.set_class_variant(i, variant)
