@@ -26,4 +26,5 @@ def main(src_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis")
+    main(sys.argv[1] if len(sys.argv) > 1 else
+         os.path.join(os.environ.get("DSS_REFERENCE_ROOT", "/root/reference"), "basis"))

@@ -26,7 +26,6 @@ extern "C" {
 #define DSS_ERR_OOM (-2)         /* device or host allocation failed */
 #define DSS_ERR_CUDA (-3)        /* CUDA runtime / launch error */
 #define DSS_ERR_NOCONV (-4)      /* SCF reached its iteration cap */
-#define DSS_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
 #define DSS_ERR_UNSUPPORTED (-6) /* e.g. angular momentum above the compiled maximum */
 
 #define DSS_BOYS_REF 0  /* the reference's truncated series (parity mode) */
