@@ -86,6 +86,12 @@ def load():
     L.dss_kernels_per_build.restype = ctypes.c_int
     L.dss_profile_build.argtypes = [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_float)]
     L.dss_profile_build.restype = ctypes.c_int
+    L.dss_time_build.argtypes = [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_float)]
+    L.dss_time_build.restype = ctypes.c_int
+    L.dss_set_persistent.argtypes = [vp, ctypes.c_int]
+    L.dss_set_persistent.restype = ctypes.c_int
+    L.dss_get_persistent.argtypes = [vp]
+    L.dss_get_persistent.restype = ctypes.c_int
     L.dss_probe_fp64_peak.argtypes = [vp, dp]
     L.dss_probe_fp64_peak.restype = ctypes.c_int
     L.dss_set_class_variant.argtypes = [vp, ctypes.c_int, ctypes.c_int]
@@ -118,6 +124,8 @@ def load():
     L.dss_load_density.restype = ctypes.c_int
     L.dss_gradient.argtypes = [vp, ctypes.c_int, ip, dp, ctypes.c_double, dp]
     L.dss_gradient.restype = ctypes.c_int
+    L.dss_eri_gradient.argtypes = [vp, dp, dp, dp, ctypes.c_int, ip, dp]
+    L.dss_eri_gradient.restype = ctypes.c_int
     L.dss_build_jk_device_noalloc.argtypes = [vp, vp, vp, vp]
     L.dss_build_jk_device_noalloc.restype = ctypes.c_int
     szt = ctypes.c_size_t
@@ -138,6 +146,10 @@ def load():
     L.dss_batch_result.restype = ctypes.c_int
     L.dss_batch_profile.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.dss_batch_profile.restype = ctypes.c_int
+    L.dss_batch_time_build.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.dss_batch_time_build.restype = ctypes.c_int
+    L.dss_batch_set_persistent.argtypes = [vp, ctypes.c_int]
+    L.dss_batch_set_persistent.restype = ctypes.c_int
     L.dss_batch_finished.argtypes = [vp, ip, ctypes.c_int, ip]
     L.dss_batch_finished.restype = ctypes.c_int
     L.dss_batch_remove.argtypes = [vp, ctypes.c_int]

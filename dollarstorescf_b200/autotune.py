@@ -10,7 +10,16 @@ shape the library offers for it and keeps the fastest:
      spills, lower occupancy), L <= 4;
   3  with about half the resident blocks, L <= 4;
   1  one warp per shell quartet with shared-memory programs (the heavy classes
-     compiled with it).
+     compiled with it);
+  4  one thread per shell quartet in persistent blocks of 8 warps that first
+     stage the class's reference-mode Boys records (35 KB per order) in shared
+     memory, L <= 2.
+
+With the per-class shapes fixed, the launch shape of the whole build is chosen
+the same way: one launch per class, or persistent grouped launches (the
+thread-per-quartet classes of L <= 2 and of L = 3..4 each in one kernel whose
+warps pull warp tasks of every class of the group from a device queue), by
+timing whole builds (dss_time_build / dss_batch_time_build).
 
 Timing is per launch with CUDA events (dss_profile_build / dss_batch_profile
 run the classes one after another on one stream), best of `repeats`.  The best
@@ -27,7 +36,7 @@ from typing import Dict, Optional
 from .engine import FockBuilder
 
 # Kernel shapes tried per class (see the module docstring).
-VARIANTS = (0, 2, 3, 1)
+VARIANTS = (0, 2, 3, 1, 4)
 
 
 def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
@@ -74,6 +83,31 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
     return choice
+
+
+def tune_launch(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 3) -> Dict[str, object]:
+    """Per-class launches or persistent grouped launches for the whole build,
+    whichever times faster (best of `repeats` whole builds each)."""
+    t = {}
+    for on in (False, True):
+        fb.set_persistent(on)
+        fb.time_build(D_ptr, J_ptr, K_ptr)
+        t[on] = min(fb.time_build(D_ptr, J_ptr, K_ptr) for _ in range(repeats))
+    best = min(t, key=t.get)
+    fb.set_persistent(best)
+    return {"persistent": best, "ms_per_class_launches": t[False], "ms_persistent": t[True]}
+
+
+def tune_batch_launch(batch, repeats: int = 3) -> Dict[str, object]:
+    """tune_launch for a dss_batch (FP64 accumulation over all live molecules)."""
+    t = {}
+    for on in (False, True):
+        batch.set_persistent(on)
+        batch.time_build()
+        t[on] = min(batch.time_build() for _ in range(repeats))
+    best = min(t, key=t.get)
+    batch.set_persistent(best)
+    return {"persistent": best, "ms_per_class_launches": t[False], "ms_persistent": t[True]}
 
 
 def tune_batch(batch, repeats: int = 2) -> Dict[str, int]:

@@ -121,6 +121,15 @@ class Batch:
         self._check(self._L.dss_batch_profile(self._h, ms))
         return [float(v) for v in ms]
 
+    def time_build(self) -> float:
+        """Device milliseconds of one whole FP64 J/K accumulation over all live molecules."""
+        ms = ctypes.c_float()
+        self._check(self._L.dss_batch_time_build(self._h, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def set_persistent(self, on: bool) -> None:
+        self._check(self._L.dss_batch_set_persistent(self._h, 1 if on else 0))
+
     def work_stats(self) -> Tuple[int, int, int]:
         """(shell quartets, primitive quartets, warp tasks) of the current composition."""
         sq, pq, wt = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()

@@ -71,7 +71,11 @@ def _class_tu(c, coop: bool) -> str:
         pb = "true" if pure else "false"
         mb = "true" if mixed else "false"
         if tiers and boys == 0 and not mixed:
-            # The plain form: register tier chosen per class by the autotuner.
+            # The plain form: register tier or shared-memory shape chosen per class
+            # by the autotuner (tier 3 = class variant 4; split launches keep tier 0).
+            if la + lb + lc + ld <= 2:  # dss_has_smem_variant
+                lines.append(f"  if (!uhf && boys == 0 && pure == {pure} && mixed == 0 && tier == 3 && a.split <= 1) "
+                             f"return dss_launch_eri_smem<{la}, {lb}, {lc}, {ld}, {pb}>(a, s);")
             for t in (2, 1):
                 lines.append(f"  if (!uhf && boys == 0 && pure == {pure} && mixed == 0 && tier == {t}) "
                              f"return eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, false, {t}>"
@@ -96,6 +100,10 @@ def _class_tu(c, coop: bool) -> str:
                              f"{{ cudaFuncGetAttributes(&fa, eri_coop_kernel<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, false>); "
                              f"return; }}")
             if tiers and boys == 0:
+                if la + lb + lc + ld <= 2:
+                    lines.append(f"  if (variant == 4 && boys == 0 && pure == {pure}) {{ "
+                                 f"cudaFuncGetAttributes(&fa, eri_jk_smem_kernel<{la}, {lb}, {lc}, {ld}, {pb}>); "
+                                 f"return; }}")
                 for t in (2, 1):
                     lines.append(f"  if (variant == {t + 1} && boys == 0 && pure == {pure}) {{ "
                                  f"cudaFuncGetAttributes(&fa, eri_jk_kernel<{la}, {lb}, {lc}, {ld}, 0, {pb}, false, "
@@ -141,6 +149,107 @@ def _class_tu(c, coop: bool) -> str:
     return "\n".join(lines) + "\n"
 
 
+# Persistent grouped launches: classes of one register budget share a kernel
+# (total angular momentum L <= 2 and 3 <= L <= 4); heavier classes keep their
+# own launches.  (boys, mixed) combinations: the plain FP64 form and the
+# mixed-precision form.
+PERSIST_GROUPS = {0: (0, 2, 6), 1: (3, 4, 4)}  # group: (L min, L max, resident blocks)
+PERSIST_COMBOS = ((0, 0), (1, 1))
+
+
+def persist_classes(classes, g):
+    lo, hi, _ = PERSIST_GROUPS[g]
+    return [c for c in classes if lo <= sum(c) <= hi]
+
+
+def _persist_tu(classes, g, boys, mixed, pure) -> str:
+    """One persistent kernel (group g, one Boys mode / form / function type)
+    and its launcher."""
+    grp = persist_classes(classes, g)
+    minb = PERSIST_GROUPS[g][2]
+    pb = "true" if pure else "false"
+    mb = "true" if mixed else "false"
+    k = f"eri_persist_g{g}_b{boys}_m{mixed}_p{pure}"
+    lines = ['#include "eri_kernels.cuh"', "#include <atomic>", ""]
+    lines.append(f"__global__ void __launch_bounds__(128, {minb}) {k}(PersistArgs p) {{")
+    lines.append("  const int lane = threadIdx.x & 31;")
+    lines.append("  const int total = p.start[p.ncls];")
+    lines.append("  for (;;) {")
+    lines.append("    int base = 0;")
+    lines.append("    if (lane == 0) base = atomicAdd(p.head, DSS_PERSIST_CHUNK);")
+    lines.append("    base = __shfl_sync(0xffffffffu, base, 0);")
+    lines.append("    if (base >= total) return;")
+    lines.append("    const int end = min(base + DSS_PERSIST_CHUNK, total);")
+    lines.append("    for (int item = base; item < end; ++item) {")
+    lines.append("      int c = 0;")
+    lines.append("      while (item >= p.start[c + 1]) ++c;")
+    lines.append("      const int task = item - p.start[c];")
+    lines.append("      switch (p.slot[c]) {")
+    for i, (la, lb, lc, ld) in enumerate(grp):
+        lines.append(f"        case {i}: eri_jk_task<{la}, {lb}, {lc}, {ld}, {boys}, {pb}, {mb}, false>"
+                     f"(p.a, p.tasks[c], task, lane, 0); break;")
+    lines.append("        default: break;")
+    lines.append("      }")
+    lines.append("    }")
+    lines.append("  }")
+    lines.append("}")
+    lines.append(f"void dss_launch_{k}(const PersistArgs& p, cudaStream_t s) {{")
+    lines.append("  static std::atomic<int> grid_dev[64] = {};")
+    lines.append("  int dev = 0;")
+    lines.append("  cudaGetDevice(&dev);")
+    lines.append("  int g = (dev >= 0 && dev < 64) ? grid_dev[dev].load() : 0;")
+    lines.append("  if (!g) {")
+    lines.append("    int per = 0, nsm = 0;")
+    lines.append(f"    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, {k}, 128, 0);")
+    lines.append("    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);")
+    lines.append("    g = (per > 0 ? per : 1) * (nsm > 0 ? nsm : 1);")
+    lines.append("    if (dev >= 0 && dev < 64) grid_dev[dev].store(g);")
+    lines.append("  }")
+    lines.append("  const long long warps = ((long long)p.start[p.ncls] + DSS_PERSIST_CHUNK - 1) / DSS_PERSIST_CHUNK;")
+    lines.append("  const long long need = (warps + 3) / 4;")
+    lines.append("  const unsigned blocks = (unsigned)(need < g ? need : g);")
+    lines.append("  if (!blocks) return;")
+    lines.append(f"  {k}<<<blocks, 128, 0, s>>>(p);")
+    lines.append("}")
+    lines.append(f"void dss_preload_{k}() {{")
+    lines.append("  cudaFuncAttributes fa;")
+    lines.append(f"  cudaFuncGetAttributes(&fa, {k});")
+    lines.append("}")
+    return "\n".join(lines) + "\n"
+
+
+def _persist_dispatch(classes) -> str:
+    lines = []
+    for g in PERSIST_GROUPS:
+        for boys, mixed in PERSIST_COMBOS:
+            for pure in (1, 0):
+                lines.append(f"void dss_launch_eri_persist_g{g}_b{boys}_m{mixed}_p{pure}(const PersistArgs& p, "
+                             f"cudaStream_t s);")
+                lines.append(f"void dss_preload_eri_persist_g{g}_b{boys}_m{mixed}_p{pure}();")
+    lines.append("void dss_preload_persist() {")
+    for g in PERSIST_GROUPS:
+        for boys, mixed in PERSIST_COMBOS:
+            for pure in (1, 0):
+                lines.append(f"  dss_preload_eri_persist_g{g}_b{boys}_m{mixed}_p{pure}();")
+    lines.append("}")
+    lines.append("int dss_persist_group(int la, int lb, int lc, int ld) {")
+    for g in PERSIST_GROUPS:
+        for i, (la, lb, lc, ld) in enumerate(persist_classes(classes, g)):
+            lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) return {g * 100 + i};")
+    lines.append("  return -1;")
+    lines.append("}")
+    lines.append("bool dss_launch_persist(int group, int boys, int pure, int mixed, const PersistArgs& p, "
+                 "cudaStream_t s) {")
+    for g in PERSIST_GROUPS:
+        for boys, mixed in PERSIST_COMBOS:
+            for pure in (1, 0):
+                lines.append(f"  if (group == {g} && boys == {boys} && mixed == {mixed} && pure == {pure}) "
+                             f"{{ dss_launch_eri_persist_g{g}_b{boys}_m{mixed}_p{pure}(p, s); return true; }}")
+    lines.append("  return false;")
+    lines.append("}")
+    return "\n".join(lines) + "\n"
+
+
 def _dispatch_tu(classes, pcls, coop) -> str:
     lines = ['#include "eri_kernels.cuh"', ""]
     for (la, lb, lc, ld) in coop:
@@ -171,6 +280,7 @@ def _dispatch_tu(classes, pcls, coop) -> str:
     for (la, lb) in pcls:
         lines.append(f"  if (la == {la} && lb == {lb}) return dss_launch_schwarz_{la}{lb}(boys, pure, a, s);")
     lines.append("}")
+    lines.append(_persist_dispatch(classes))
     lines.append("void dss_launch_eri_jk(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, "
                  "int tier, const EriArgs& a, cudaStream_t s) {")
     for (la, lb, lc, ld) in classes:
@@ -197,14 +307,16 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     boys_data = os.path.join(GEN, "boys_cell_data.cu")
     gen_stamp = os.path.join(GEN, "stamp")
     want = _stamp([os.path.join(CSRC, "gen_eri.py"), os.path.join(CSRC, "gen_boys_tab.py"),
-                   os.path.join(CSRC, "gen_coop.py")], str(lmax))
+                   os.path.join(CSRC, "gen_coop.py"), os.path.join(CSRC, "gen_grad.py")], str(lmax))
     have = open(gen_stamp).read() if os.path.isfile(gen_stamp) else ""
     sph_tab = os.path.join(GEN, "sph_tab.h")
     coop_gen = os.path.join(GEN, "coop_gen.cuh")
-    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, boys_data, sph_tab, coop_gen)):
+    grad_gen = os.path.join(GEN, "grad_gen.cuh")
+    if have != want or not all(os.path.isfile(x) for x in (eri_gen, boys_tab, boys_data, sph_tab, coop_gen, grad_gen)):
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_eri.py"), eri_gen, str(lmax)])
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_boys_tab.py"), boys_tab, boys_data])
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_coop.py"), coop_gen, str(lmax)])
+        subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_grad.py"), grad_gen, str(lmax)])
         with open(gen_stamp, "w") as f:
             f.write(want)
     classes, pcls, coop = _classes(lmax)
@@ -213,6 +325,15 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
         p = os.path.join(GEN, "eri_class_%d%d%d%d.cu" % c)
         _write_if_changed(p, _class_tu(c, c in coop))
         units.append(p)
+    persist_units = set()
+    for g in PERSIST_GROUPS:
+        for boys, mixed in PERSIST_COMBOS:
+            for pure in (1, 0):
+                name = f"eri_persist_g{g}_b{boys}_m{mixed}_p{pure}.cu"
+                p = os.path.join(GEN, name)
+                _write_if_changed(p, _persist_tu(classes, g, boys, mixed, pure))
+                units.append(p)
+                persist_units.add(name)
     p = os.path.join(GEN, "eri_dispatch.cu")
     _write_if_changed(p, _dispatch_tu(classes, pcls, coop))
     units.append(p)
@@ -221,7 +342,7 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
         if name.endswith(".cu"):
             units.append(os.path.join(CSRC, name))
     headers = [os.path.join(CSRC, n) for n in sorted(os.listdir(CSRC)) if n.endswith((".cuh", ".h"))]
-    headers += [eri_gen, boys_tab, sph_tab, coop_gen, os.path.join(INCLUDE, "dss.h")]
+    headers += [eri_gen, boys_tab, sph_tab, coop_gen, grad_gen, os.path.join(INCLUDE, "dss.h")]
     all_stamp = _stamp(headers, " ".join(CFLAGS + ARCH))
     # The generated class units only see the kernel headers.
     kernel_headers = [os.path.join(CSRC, n) for n in ("eri_kernels.cuh", "common.cuh", "boys.cuh")]
@@ -236,7 +357,7 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
         base = os.path.basename(src)
         if base in coop_units:
             hdr = coop_stamp
-        elif base.startswith("eri_class_"):
+        elif base.startswith("eri_class_") or base in persist_units:
             hdr = kernel_stamp
         else:
             hdr = all_stamp
@@ -256,8 +377,11 @@ def build(lmax: int = 2, jobs: int = 0, verbose: bool = False) -> str:
     jobs = jobs or max(1, os.cpu_count() or 1)
     with ThreadPoolExecutor(jobs) as ex:
         objs = list(ex.map(compile_one, units))
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread"]
+    # Link beside the library and rename, so that a reader never sees a partly written file.
+    tmp = LIB + ".tmp"
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static", "-lpthread"]
     subprocess.check_call(cmd)
+    os.replace(tmp, LIB)
     return LIB
 
 

@@ -1340,6 +1340,57 @@ int dss_batch_profile(dss_batch* b, float* ms) {
   return DSS_OK;
 }
 
+int dss_batch_time_build(dss_batch* b, float* ms) {
+  if (!b || !ms) return DSS_ERR_INVALID;
+  b->err.clear();
+  *ms = 0.0f;
+  cudaSetDevice(b->ctx->opts.device);
+  if (b->dirty) {
+    const int rc = rebuild(b);
+    if (rc != DSS_OK) return rc;
+  }
+  const int nb = (int)b->slot_mol.size();
+  if (!nb) return DSS_OK;
+  dss_ctx* ctx = b->ctx;
+  cudaStream_t s = ctx->stream;
+  DevBuf<int> all;
+  if (all.resize(nb) != cudaSuccess) return bfail(b, DSS_ERR_OOM, "dss_batch_time_build: allocation");
+  std::vector<int> ones(nb, 1);
+  cudaMemcpyAsync(all.ptr, ones.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s);
+  BatchView v = view(b, all.ptr);
+  const long long nn = (long long)b->nmax * b->nmax;
+  k_prep<<<grid2(nn, nb), 256, 0, s>>>(v);
+  ctx->d_mol_active = all.ptr;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  BuildMode bm;
+  bm.boys = ctx->opts.boys_mode;
+  bm.no_zero = true;
+  cudaEventRecord(e0, s);
+  int rc = dss_enqueue_jk(ctx, b->arena.ptr, b->arena.ptr, b->arena.ptr, nullptr, &bm);
+  cudaEventRecord(e1, s);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (rc == DSS_OK && e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->d_mol_active = b->d_active.ptr;
+  if (rc != DSS_OK) return bfail(b, rc, "dss_batch_time_build: launch failed");
+  if (e != cudaSuccess) return bfail(b, DSS_ERR_CUDA, std::string("dss_batch_time_build: ") + cudaGetErrorString(e));
+  return DSS_OK;
+}
+
+int dss_batch_set_persistent(dss_batch* b, int on) {
+  if (!b) return DSS_ERR_INVALID;
+  const int rc = dss_set_persistent(b->ctx, on);
+  if (rc == DSS_OK && b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->eager_ran = false;
+  return rc;
+}
+
 int dss_batch_finished(const dss_batch* b, int* handles, int cap, int* count) {
   if (!b || !count || (cap > 0 && !handles)) return DSS_ERR_INVALID;
   const int n = (int)b->last_finished.size();

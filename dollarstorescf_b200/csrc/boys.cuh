@@ -27,6 +27,10 @@
 
 #define DSS_BOYS_REF 0
 #define DSS_BOYS_FAST 1
+// Reference values as DSS_BOYS_REF, with the block-A cell records of orders
+// 0..L read from dynamic shared memory (dss_boys_smem_stage); only kernels that
+// stage them may instantiate this mode.
+#define DSS_BOYS_REF_SMEM 2
 
 #define DSS_PI_REF 3.14159265358979
 
@@ -328,7 +332,27 @@ __device__ __forceinline__ void boys_ref_walk(double x, double* F) {
 // series itself (a separate function) runs only for x < 1/32 (cell 0 holds
 // several breakpoints) and within 4e-14 (relative) of a breakpoint, where the
 // rounding of the reference's own sum decides its stop.
+// Block-A records of orders 0..L staged in shared memory: record r (order-major,
+// as in the global table) keeps its four 16-byte chunks at r*4 + ((j + (r >> 1)) & 3),
+// so the first chunks of random records spread over all eight 16-byte bank groups.
+extern __shared__ __align__(16) double2 dss_boys_smem[];
+
+__device__ __forceinline__ int dss_boys_smem_slot(int r, int j) { return r * 4 + ((j + (r >> 1)) & 3); }
+
+// Copies the block-A records of orders 0..L into dss_boys_smem (every thread of
+// the block takes part; ends with a block barrier).
 template <int L>
+__device__ __forceinline__ void dss_boys_smem_stage(const double* __restrict__ cells) {
+  const double2* src = reinterpret_cast<const double2*>(cells);
+  const int nchunk = (L + 1) * DSS_BOYS_NCELL * 4;
+  for (int i = threadIdx.x; i < nchunk; i += blockDim.x) dss_boys_smem[dss_boys_smem_slot(i >> 2, i & 3)] = __ldg(src + i);
+  __syncthreads();
+}
+
+template <int L>
+__host__ __device__ constexpr size_t dss_boys_smem_bytes() { return (size_t)(L + 1) * DSS_BOYS_NCELL * 64; }
+
+template <int L, bool SMEM = false>
 __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double* __restrict__ cells) {
   static_assert(L < DSS_BOYS_NMC, "cell records too narrow for this order");
   // Orders m < m_lo take the asymptotic form (x > 1.1 m + 25; the thresholds
@@ -360,7 +384,19 @@ __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double
   for (int m = 0; m <= L; ++m) {
     if (m < m_lo) continue;
     const double2* r = reinterpret_cast<const double2*>(cells) + ((size_t)m * DSS_BOYS_NCELL + k) * 4;
-    double2 c01 = __ldg(r), c23 = __ldg(r + 1), c45 = __ldg(r + 2), c6b = __ldg(r + 3);
+    double2 c01, c23, c45, c6b;
+    if constexpr (SMEM) {
+      const int rec = m * DSS_BOYS_NCELL + k;
+      c01 = dss_boys_smem[dss_boys_smem_slot(rec, 0)];
+      c23 = dss_boys_smem[dss_boys_smem_slot(rec, 1)];
+      c45 = dss_boys_smem[dss_boys_smem_slot(rec, 2)];
+      c6b = dss_boys_smem[dss_boys_smem_slot(rec, 3)];
+    } else {
+      c01 = __ldg(r);
+      c23 = __ldg(r + 1);
+      c45 = __ldg(r + 2);
+      c6b = __ldg(r + 3);
+    }
     const double b = c6b.y;
     if (x > b) {  // the piece past the cell's breakpoint, same index in block B
       r += (size_t)DSS_BOYS_NMC * DSS_BOYS_NCELL * 4;
@@ -406,7 +442,10 @@ __device__ __forceinline__ void boys_ref(double x, double* F, const double* __re
 
 template <int BOYS, int L>
 __device__ __forceinline__ void boys_eval(double x, double* F, const double* __restrict__ cells) {
-  if constexpr (BOYS == DSS_BOYS_REF) {
+  if constexpr (BOYS == DSS_BOYS_REF_SMEM) {
+    static_assert(L <= DSS_BOYS_CELL_LMAX && L < DSS_BOYS_NMC, "shared-memory records need the cell table");
+    boys_ref_cells<L, true>(x, F, cells);
+  } else if constexpr (BOYS == DSS_BOYS_REF) {
     boys_ref<L>(x, F, cells);
   } else {
     boys_fast<L>(x, F);

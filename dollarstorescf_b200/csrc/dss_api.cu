@@ -466,6 +466,20 @@ int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out, bool with_tas
   return DSS_OK;
 }
 
+void dss_pair_alphas(const dss_ctx* ctx, std::vector<double>* alpha) {
+  const BasisHost& B = ctx->basis;
+  alpha->clear();
+  for (size_t q = 0; q < ctx->h_pair_a.size(); ++q) {
+    const int a = ctx->h_pair_a[q], b = ctx->h_pair_b[q];
+    const double dx = B.xyz[3 * a] - B.xyz[3 * b], dy = B.xyz[3 * a + 1] - B.xyz[3 * b + 1],
+                 dz = B.xyz[3 * a + 2] - B.xyz[3 * b + 2];
+    const double ab2 = dx * dx + dy * dy + dz * dz;
+    for (int i = 0; i < B.nprim[a]; ++i)
+      for (int j = 0; j < B.nprim[b]; ++j)
+        if (keep_prim_pair(B, a, i, b, j, ab2, ctx->opts.primitive_threshold)) alpha->push_back(B.exps[B.prim0[a] + i]);
+  }
+}
+
 void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out,
                      const std::vector<long long>* pp_offset) {
   PairSet& P = *out;
@@ -736,15 +750,36 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     return a.la + a.lb + a.lc + a.ld > b.la + b.lb + b.lc + b.ld;
   });
   const bool fork = events == nullptr;
+  const int eboys = mode->mixed ? DSS_BOYS_FAST : mode->boys;
+  // Persistent grouped launches (dss_set_persistent): the thread-per-quartet,
+  // unsplit classes of each register group share one kernel fed by a device
+  // work queue; warp-cooperative and split classes keep their own launches.
+  PersistArgs pg[2];
+  int npg[2] = {0, 0};
+  std::vector<int> single;
+  const bool persist = ctx->persist && !mode->uhf && !events && ctx->d_persist_head.ptr &&
+                       ((eboys == DSS_BOYS_REF && !mode->mixed) || (eboys == DSS_BOYS_FAST && mode->mixed));
+  for (int ci : order) {
+    const ClassTasks& ct = ctx->tasks[ci];
+    const int gid = persist ? dss_persist_group(ct.la, ct.lb, ct.lc, ct.ld) : -1;
+    if (gid < 0 || ct.variant == 1 || ct.split > 1) {
+      single.push_back(ci);
+      continue;
+    }
+    PersistArgs& p = pg[gid / 100];
+    int& k = npg[gid / 100];
+    if (k == 0) p.start[0] = 0;
+    p.tasks[k] = ct.d_tasks.ptr;
+    p.slot[k] = gid % 100;
+    p.start[k + 1] = p.start[k] + ct.ntasks;
+    ++k;
+  }
   if (fork) {
     DSS_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
     for (int i = 0; i < dss_ctx::kSideStreams; ++i) DSS_CUDA(cudaStreamWaitEvent(ctx->side[i], ctx->fork_ev, 0));
   }
   int slot = 0;
-  for (int ci : order) {
-    ClassTasks& ct = ctx->tasks[ci];
-    cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
-    EriArgs a{};
+  auto common_args = [&](EriArgs& a) {
     if (batch) {
       a.sh_mbase = ctx->d_sh_mbase.ptr;
       a.sh_jbase = ctx->d_sh_jbase.ptr;
@@ -756,9 +791,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
       a.sh_nsm = ctx->d_sh_nsm.ptr;
       a.mol_active = ctx->d_mol_active;
     }
-    a.tasks = ct.d_tasks.ptr;
-    a.ntasks = ct.ntasks;
-    a.split = ct.split;
+    a.split = 1;
     a.pair_a = ctx->d_pair_a.ptr;
     a.pair_b = ctx->d_pair_b.ptr;
     a.pair_pp0 = ctx->d_pair_pp0.ptr;
@@ -779,6 +812,31 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     a.Da = mode->Da;
     a.Db = mode->Db;
     a.K2 = mode->K2;
+  };
+  if (npg[0] || npg[1]) {
+    // The queue heads are zeroed on each group's stream before its launch.
+    for (int g = 0; g < 2; ++g) {
+      if (!npg[g]) continue;
+      PersistArgs& p = pg[g];
+      p.a = EriArgs{};
+      common_args(p.a);
+      p.ncls = npg[g];
+      p.head = ctx->d_persist_head.ptr + g;
+      cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
+      DSS_CUDA(cudaMemsetAsync(p.head, 0, sizeof(int), st));
+      if (!dss_launch_persist(g, eboys, ctx->pure, mode->mixed, p, st))
+        return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_enqueue_jk: no persistent kernel for this form");
+      DSS_CUDA(cudaGetLastError());
+    }
+  }
+  for (int ci : single) {
+    ClassTasks& ct = ctx->tasks[ci];
+    cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
+    EriArgs a{};
+    common_args(a);
+    a.tasks = ct.d_tasks.ptr;
+    a.ntasks = ct.ntasks;
+    a.split = ct.split;
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci], st));
     dss_launch_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, mode->mixed ? DSS_BOYS_FAST : mode->boys, ctx->pure,
                            mode->mixed, mode->uhf ? 1 : 0, ct.variant, a, st);
@@ -884,7 +942,7 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* sq, long long*
 }
 
 int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
-  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 3) return DSS_ERR_INVALID;
+  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 4) return DSS_ERR_INVALID;
   if (ctx->class_variant.size() < (size_t)DSS_N_QUARTET_CLASSES) ctx->class_variant.assign(DSS_N_QUARTET_CLASSES, -1);
   static const int kL[][4] = {
 #define DSS_CLASS_L2(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_},
@@ -893,8 +951,10 @@ int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
   };
   if (variant == 1 && !dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]))
     return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: no warp-cooperative kernel for this class");
-  if (variant >= 2 && !dss_has_tiers(kL[i][0] + kL[i][1] + kL[i][2] + kL[i][3]))
+  if ((variant == 2 || variant == 3) && !dss_has_tiers(kL[i][0] + kL[i][1] + kL[i][2] + kL[i][3]))
     return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: this class has one register tier");
+  if (variant == 4 && !dss_has_smem_variant(kL[i][0] + kL[i][1] + kL[i][2] + kL[i][3]))
+    return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: no shared-memory Boys shape for this class");
   ctx->class_variant[i] = variant;
   if ((size_t)i < ctx->tasks.size()) {
     ClassTasks& ct = ctx->tasks[i];
@@ -917,6 +977,52 @@ int dss_kernels_per_build(const dss_ctx* ctx) {
   for (const auto& ct : ctx->tasks)
     if (ct.ntasks) ++k;
   return k + 2;  // + the two symmetrisations
+}
+
+// Loads every persistent kernel (under lazy module loading), so that their first
+// launches allocate no code memory (generated dispatch unit).
+extern "C++" void dss_preload_persist();
+
+int dss_set_persistent(dss_ctx* ctx, int on) {
+  if (!ctx) return DSS_ERR_INVALID;
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  if (on && !ctx->d_persist_head.ptr) {
+    if (ctx->d_persist_head.resize(2) != cudaSuccess)
+      return dss_fail(ctx, DSS_ERR_OOM, "dss_set_persistent: device allocation failed");
+    DSS_CUDA(cudaMemsetAsync(ctx->d_persist_head.ptr, 0, 2 * sizeof(int), ctx->stream));
+  }
+  if (on) dss_preload_persist();
+  ctx->persist = on != 0;
+  return DSS_OK;
+}
+
+int dss_get_persistent(const dss_ctx* ctx) { return ctx && ctx->persist ? 1 : 0; }
+
+int dss_time_build(dss_ctx* ctx, const double* D, double* J, double* K, float* ms) {
+  if (!ctx || !ms) return DSS_ERR_INVALID;
+  if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_time_build: no basis set");
+  DSS_CUDA(cudaSetDevice(ctx->opts.device));
+  const int n = ctx->nbf;
+  const size_t nn = (size_t)n * n;
+  if (ctx->Jacc.resize(nn) != cudaSuccess || ctx->Kacc.resize(nn) != cudaSuccess)
+    return dss_fail(ctx, DSS_ERR_OOM, "dss_time_build: device allocation failed");
+  cudaEvent_t e0, e1;
+  DSS_CUDA(cudaEventCreate(&e0));
+  DSS_CUDA(cudaEventCreate(&e1));
+  cudaEventRecord(e0, ctx->stream);
+  int rc = dss_enqueue_jk(ctx, D, ctx->Jacc.ptr, ctx->Kacc.ptr);
+  cudaEventRecord(e1, ctx->stream);
+  if (rc == DSS_OK) {
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((nn + threads - 1) / threads);
+    if (J) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Jacc.ptr, J, nullptr, n);
+    if (K) symmetrize_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->Kacc.ptr, K, nullptr, n);
+    rc = dss_cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "dss_time_build");
+  }
+  if (rc == DSS_OK) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }
 
 int dss_profile_build(dss_ctx* ctx, const double* D, double* J, double* K, float* ms) {

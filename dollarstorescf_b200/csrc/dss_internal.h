@@ -117,6 +117,9 @@ struct dss_ctx {
   std::vector<int> class_pair0, class_pair1;
   std::vector<ClassTasks> tasks;
   std::vector<int> class_variant;  // per class: -1 default, 0 thread, 1 warp-cooperative
+  // Persistent grouped launches (dss_set_persistent) and their queue heads.
+  bool persist = false;
+  DevBuf<int> d_persist_head;
   std::vector<int> h_pair_mol;
 
   // Batch mode (nmol > 0, set by the batch engine): per-shell matrix offsets
@@ -212,6 +215,9 @@ int dss_pairs_make(dss_ctx* ctx, const BasisHost& B, PairSet* out, bool with_tas
 // and its p0 index that pool.
 void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector<int>& shell_offset, PairSet* out,
                      const std::vector<long long>* pp_offset = nullptr);
+// Exponent of the first shell's primitive of every primitive pair of the
+// context's basis (one molecule), in the order of its device primitive pairs.
+void dss_pair_alphas(const dss_ctx* ctx, std::vector<double>* alpha);
 // Makes B and P the context's basis: uploads, class ranges, work lists.
 int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks = nullptr);
 int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
@@ -265,5 +271,11 @@ struct BuildMode {
 // around the launch of class i.  mode == NULL: the context's Boys mode, FP64.
 int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cudaEvent_t* events = nullptr,
                    const BuildMode* mode = nullptr);
+// Analytic two-electron gradient of the context's basis (one molecule) into
+// grad_host[3 natom] (overwritten): densities dense n x n on the device, D the
+// total, X (and Y) the exchange densities with factor xfac (RHF: X = D, Y = NULL,
+// 1/4; UHF: D_alpha, D_beta, 1/2); shell_atom[s] the nucleus of shell s (host).
+int dss_eri_gradient_dense(dss_ctx* ctx, const double* D_dev, const double* X_dev, const double* Y_dev, double xfac,
+                           int natom, const int* shell_atom, double* grad_host);
 // Per shell-pair block maximum of |D| (dense n x n, device) into dmax [nshell^2].
 void dss_block_max(dss_ctx* ctx, const double* D, float* dmax);

@@ -19,6 +19,8 @@
 // Jacc[i][j] sums, shared by the whole warp (same bra pair), are reduced with
 // warp shuffles before a single atomic per element.
 #pragma once
+#include <atomic>
+
 #include "common.cuh"
 #include "eri_gen.cuh"
 
@@ -230,17 +232,17 @@ __device__ __forceinline__ void digest_k(const double* I, double s, const double
   }
 }
 
+// One warp task (warp = task index): the bra pair against up to 32 ket pairs,
+// one per lane, evaluated and digested.  slice: the bra-primitive slice of a
+// split launch (a.split > 1), else 0.
 // UHF = true: the unrestricted variant (one molecule): J from a.D = D_a + D_b,
 // K from a.Da into a.K and from a.Db into a.K2, from one evaluation of the integrals.
-// TIER: register tier (dss_min_blocks_tier).
-template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false, bool UHF = false, int TIER = 0>
-__global__ void __launch_bounds__(128, dss_min_blocks_tier(LA + LB + LC + LD, TIER)) eri_jk_kernel(EriArgs a) {
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED, bool UHF>
+__device__ __forceinline__ void eri_jk_task(const EriArgs& a, const int4* __restrict__ tasks, int warp, int lane,
+                                            int slice) {
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE);
   constexpr int NC = dss_nfunc(LC, PURE), ND = dss_nfunc(LD, PURE);
-  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (warp >= a.ntasks) return;  // uniform per warp
-  const int4 t = __ldg(a.tasks + warp);
+  const int4 t = __ldg(tasks + warp);
   bool active = lane < t.z;
   const int bra = t.x;
   const int ket = t.y + (active ? lane : 0);
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(128, dss_min_blocks_tier(LA + LB + LC + LD, TI
   // so every slice digests its partial sum and J/K add up to the full quartet.
   int bpp0 = __ldg(a.pair_pp0 + bra), bnpp = __ldg(a.pair_npp + bra);
   if (a.split > 1) {
-    const int lo = bnpp * (int)blockIdx.y / a.split, hi = bnpp * ((int)blockIdx.y + 1) / a.split;
+    const int lo = bnpp * slice / a.split, hi = bnpp * (slice + 1) / a.split;
     if (lo == hi) return;  // uniform per warp
     bpp0 += lo;
     bnpp = hi - lo;
@@ -356,6 +358,80 @@ __global__ void __launch_bounds__(128, dss_min_blocks_tier(LA + LB + LC + LD, TI
   }
 }
 
+// Thread per shell quartet, warp per task.  TIER: register tier (dss_min_blocks_tier).
+template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false, bool UHF = false, int TIER = 0>
+__global__ void __launch_bounds__(128, dss_min_blocks_tier(LA + LB + LC + LD, TIER)) eri_jk_kernel(EriArgs a) {
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (warp >= a.ntasks) return;  // uniform per warp
+  eri_jk_task<LA, LB, LC, LD, BOYS, PURE, MIXED, UHF>(a, a.tasks, warp, threadIdx.x & 31, (int)blockIdx.y);
+}
+
+// The shared-memory Boys shape (class variant 4; plain form, reference Boys,
+// total angular momentum L <= 2, unsplit launches): persistent blocks of
+// DSS_SMEM_WARPS warps first copy the block-A cell records of orders 0..L
+// (35 KB per order) into shared memory with coalesced 16-byte loads, then walk
+// the warp tasks with a grid stride; each lane's Boys lookups read the staged
+// records instead of gathering them through L1/L2.  Resident blocks per SM are
+// set by the staged bytes: 4 / 3 / 2 for L = 0 / 1 / 2.
+#define DSS_SMEM_WARPS 8
+__host__ __device__ constexpr int dss_smem_min_blocks(int L) { return L == 0 ? 4 : (L == 1 ? 3 : 2); }
+__host__ __device__ constexpr bool dss_has_smem_variant(int L) { return L <= 2; }
+
+template <int LA, int LB, int LC, int LD, bool PURE>
+__global__ void __launch_bounds__(32 * DSS_SMEM_WARPS, dss_smem_min_blocks(LA + LB + LC + LD))
+    eri_jk_smem_kernel(EriArgs a) {
+  dss_boys_smem_stage<LA + LB + LC + LD>(a.boys_cell);
+  const int lane = threadIdx.x & 31;
+  for (int w = (int)blockIdx.x * DSS_SMEM_WARPS + (int)(threadIdx.x >> 5); w < a.ntasks;
+       w += (int)gridDim.x * DSS_SMEM_WARPS)
+    eri_jk_task<LA, LB, LC, LD, DSS_BOYS_REF_SMEM, PURE, false, false>(a, a.tasks, w, lane, 0);
+}
+
+// Persistent grouped launch: one kernel runs the warp tasks of several classes
+// (a group of classes with one register budget) from a device work queue.
+// Items are the classes' warp tasks concatenated in launch order (highest
+// total angular momentum first); each warp takes DSS_PERSIST_CHUNK consecutive
+// items per atomicAdd on the queue head and runs each through its class's task
+// body, so the classes of a group share the SMs and no class waits for another
+// class's launch to drain.
+#define DSS_PERSIST_MAX 10
+#define DSS_PERSIST_CHUNK 4
+struct PersistArgs {
+  EriArgs a;                       // common arguments (a.tasks / a.ntasks unused)
+  const int4* tasks[DSS_PERSIST_MAX];
+  int start[DSS_PERSIST_MAX + 1];  // class k owns items [start[k], start[k + 1])
+  int slot[DSS_PERSIST_MAX];       // class k's position in the group's class list
+  int ncls;
+  int* head;                       // queue head, zeroed before the launch
+};
+
+// Host launcher of the shared-memory Boys shape: sets the kernel's dynamic
+// shared-memory limit and reads its resident blocks per SM once per device, and
+// launches at most that many blocks per SM.
+template <int LA, int LB, int LC, int LD, bool PURE>
+inline void dss_launch_eri_smem(const EriArgs& a, cudaStream_t s) {
+  constexpr int L = LA + LB + LC + LD;
+  const size_t smem = dss_boys_smem_bytes<L>();
+  static std::atomic<int> grid_dev[64] = {};  // resident blocks x SMs, per device (0: not yet read)
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int g = (dev >= 0 && dev < 64) ? grid_dev[dev].load() : 0;
+  if (!g) {
+    cudaFuncSetAttribute(eri_jk_smem_kernel<LA, LB, LC, LD, PURE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    int per = 0, nsm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, eri_jk_smem_kernel<LA, LB, LC, LD, PURE>,
+                                                  32 * DSS_SMEM_WARPS, smem);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    g = (per > 0 ? per : 1) * (nsm > 0 ? nsm : 1);
+    if (dev >= 0 && dev < 64) grid_dev[dev].store(g);
+  }
+  const long long need = ((long long)a.ntasks + DSS_SMEM_WARPS - 1) / DSS_SMEM_WARPS;
+  const unsigned blocks = (unsigned)(need < g ? need : g);
+  if (!blocks) return;
+  eri_jk_smem_kernel<LA, LB, LC, LD, PURE><<<blocks, 32 * DSS_SMEM_WARPS, smem, s>>>(a);
+}
+
 // Schwarz factors Q_ab = sqrt(max_ij |(ij|ij)|) for the pairs of one class: one
 // warp per shell pair, the lanes splitting the bra primitive pairs (each lane
 // sums its bra primitive pairs against every ket primitive pair), the diagonal
@@ -399,11 +475,17 @@ DSS_FOR_EACH_CLASS(DSS_DECLARE_LAUNCHERS)
 void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a, cudaStream_t s);
 // variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class);
 // 2, 3: one thread per quartet in register tier 1, 2 (plain form: reference Boys,
-// FP64; other forms run tier 0).  uhf = 1: the unrestricted variant (thread per
+// FP64; other forms run tier 0); 4: the shared-memory Boys shape (plain form,
+// L <= 2; split launches and other forms run tier 0).  uhf = 1: the unrestricted variant (thread per
 // quartet, reference Boys only).
 void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, int variant,
                             const EriArgs& a, cudaStream_t s);
 bool dss_has_coop(int la, int lb, int lc, int ld);
+// Persistent grouped launches: group * 100 + the class's slot in its group, or
+// -1 for a class that has none; the launcher of a group's kernel (false when
+// the group has no kernel for this Boys mode / form).
+int dss_persist_group(int la, int lb, int lc, int ld);
+bool dss_launch_persist(int group, int boys, int pure, int mixed, const PersistArgs& p, cudaStream_t s);
 // Loads the FP64 kernel of a plain build of the class (variant as above) if the
 // CUDA runtime loads modules lazily, so that its first launch allocates nothing.
 void dss_preload_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant);

@@ -6,16 +6,12 @@
 //
 // with the density D, the energy-weighted density W = sum_s sum_occ eps_i C_i C_i^T
 // (RHF: twice the alpha sum) and the two-particle density of the converged
-// determinant.  Every term differentiates integrals at fixed D and W, so this
-// function evaluates the fixed-density expression
-//
-//   E_fix(R) = tr(D H(R)) + E_2e[D](R) - tr(W S(R)) + V_nn(R)
-//
-// at R +- h along each nuclear coordinate (the basis functions move with their
-// nucleus) with the device one-electron kernels and one device J/K build per
-// point, and takes the central difference.  It is not an analytic derivative:
-// the truncation error is O(h^2) (h = 1e-4 bohr: ~1e-9 Eh/bohr), and each point
-// costs a basis set-up and a build (6 natom of them).
+// determinant.  The two-electron term is analytic: derivative ERIs fused with the
+// two-particle-density digest on the device (dss_eri_gradient_dense,
+// eri_gradient.cu).  The one-electron terms differentiate S, T and V at fixed D
+// and W by central differences of the device one-electron integrals (the basis
+// functions move with their nucleus; step h, truncation error O(h^2): h = 1e-4
+// bohr gives ~1e-9 Eh/bohr), 6 natom one-electron evaluations and no J/K build.
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -34,13 +30,6 @@ double trace_dense_packed(const std::vector<double>& A, const std::vector<double
       const double x = Xp[(size_t)j * (j + 1) / 2 + i];
       s += (i == j ? 1.0 : 2.0) * A[(size_t)i * n + j] * x;
     }
-  return s;
-}
-
-// tr(A (Acc + Acc^T)) for dense A (symmetric) and an accumulator Acc.
-double trace_sym_acc(const std::vector<double>& A, const std::vector<double>& acc, int n) {
-  double s = 0.0;
-  for (size_t t = 0; t < (size_t)n * n; ++t) s += 2.0 * A[t] * acc[t];
   return s;
 }
 
@@ -90,20 +79,9 @@ extern "C" int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double*
         W[(size_t)i * n + j] += occ * w;
       }
   }
-  // A private context for the displaced geometries (the caller's basis stays).
-  dss_opts o = ctx->opts;
-  o.schwarz_threshold = std::min(o.schwarz_threshold, 1e-15);  // no quartet flips in or out between points
-  dss_ctx* g = nullptr;
-  int rc = dss_create(&g, &o);
-  if (rc != DSS_OK) return dss_fail(ctx, rc, std::string("dss_gradient: ") + dss_last_error(nullptr));
-  struct Guard {
-    dss_ctx* c;
-    ~Guard() { dss_destroy(c); }
-  } guard{g};
-  cudaStream_t s = g->stream;
-  DevBuf<double> dmat, acc, pk;
-  if (dmat.resize(3 * n2) != cudaSuccess || acc.resize(3 * n2) != cudaSuccess ||
-      pk.resize((size_t)n * (n + 1)) != cudaSuccess)
+  cudaStream_t s = ctx->stream;
+  DevBuf<double> dmat, pk;
+  if (dmat.resize(3 * n2) != cudaSuccess || pk.resize((size_t)n * (n + 1)) != cudaSuccess)
     return dss_fail(ctx, DSS_ERR_OOM, "dss_gradient: device allocation failed");
   double* dDt = dmat.ptr;
   double* dDa = dmat.ptr + n2;
@@ -112,69 +90,38 @@ extern "C" int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double*
   if (uhf && e == cudaSuccess) e = cudaMemcpyAsync(dDa, Ds[0].data(), n2 * 8, cudaMemcpyHostToDevice, s);
   if (uhf && e == cudaSuccess) e = cudaMemcpyAsync(dDb, Ds[1].data(), n2 * 8, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return dss_fail(ctx, DSS_ERR_CUDA, std::string("dss_gradient: ") + cudaGetErrorString(e));
+  // Two-electron part: analytic.
+  std::vector<double> g2(3 * (size_t)natom, 0.0);
+  int rc = uhf ? dss_eri_gradient_dense(ctx, dDt, dDa, dDb, 0.5, natom, owner.data(), g2.data())
+           : dss_eri_gradient_dense(ctx, dDt, dDt, nullptr, 0.25, natom, owner.data(), g2.data());
+  if (rc != DSS_OK) return rc;
+  // One-electron part: E_1(R) = tr(D H(R)) - tr(W S(R)) + V_nn(R) at displaced nuclei.
   const size_t np = (size_t)n * (n + 1) / 2;
-  std::vector<double> Sp(np), Hp(np), Jh(n2), Kh(n2), K2h(n2);
+  std::vector<double> Sp(np), Hp(np);
   std::vector<double> xyz(xyz_bohr, xyz_bohr + 3 * (size_t)natom);
-  // E_fix at the geometry with nucleus a moved by delta along axis d.
-  auto energy = [&](int a, int d, double delta, double* E) -> int {
+  auto energy1 = [&](int a, int d, double delta, double* E) -> int {
     BasisHost B = B0;
     for (int q = 0; q < ns; ++q)
       if (owner[q] == a) B.xyz[3 * q + d] += delta;
     xyz[3 * a + d] = xyz_bohr[3 * a + d] + delta;
-    int r = dss_setup_pairs(g, std::move(B));
-    if (r != DSS_OK) return r;
     std::string err;
-    r = dss_one_electron_device(s, g->basis, natom, Z, xyz.data(), pk.ptr, pk.ptr + np, nullptr, &err, &g->oe_scratch);
-    if (r != DSS_OK) return r;
-    BuildMode m;
-    m.boys = o.boys_mode;
-    if (uhf && o.boys_mode == DSS_BOYS_REF) {
-      m.uhf = true;
-      m.Da = dDa;
-      m.Db = dDb;
-      m.K2 = acc.ptr + 2 * n2;
-    }
-    r = dss_enqueue_jk(g, uhf && !m.uhf ? dDa : dDt, acc.ptr, acc.ptr + n2, nullptr, &m);
-    if (r != DSS_OK) return r;
+    int r = dss_one_electron_device(s, B, natom, Z, xyz.data(), pk.ptr, pk.ptr + np, nullptr, &err, &ctx->oe_scratch);
+    if (r != DSS_OK) return dss_fail(ctx, r, "dss_gradient: one-electron integrals: " + err);
     cudaError_t ce = cudaMemcpyAsync(Sp.data(), pk.ptr, np * 8, cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(Hp.data(), pk.ptr + np, np * 8, cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(Jh.data(), acc.ptr, n2 * 8, cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(Kh.data(), acc.ptr + n2, n2 * 8, cudaMemcpyDeviceToHost, s);
-    if (uhf && m.uhf && ce == cudaSuccess)
-      ce = cudaMemcpyAsync(K2h.data(), acc.ptr + 2 * n2, n2 * 8, cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    if (ce != cudaSuccess) return DSS_ERR_CUDA;
-    double E2;
-    if (!uhf) {
-      // J[Dt], K[Dt]: E_2e = tr(Dt J)/2 - tr(Dt K)/4.
-      E2 = 0.5 * trace_sym_acc(Dt, Jh, n) - 0.25 * trace_sym_acc(Dt, Kh, n);
-    } else if (m.uhf) {
-      // J[Dt], K[Da], K[Db]: E_2e = tr(Dt J)/2 - (tr(Da Ka) + tr(Db Kb))/2.
-      E2 = 0.5 * trace_sym_acc(Dt, Jh, n) - 0.5 * (trace_sym_acc(Ds[0], Kh, n) + trace_sym_acc(Ds[1], K2h, n));
-    } else {
-      // Accurate Boys mode: J and K of each spin from two builds.
-      const std::vector<double> Ja = Jh, Ka = Kh;
-      r = dss_enqueue_jk(g, dDb, acc.ptr, acc.ptr + n2, nullptr, &m);
-      if (r != DSS_OK) return r;
-      ce = cudaMemcpyAsync(Jh.data(), acc.ptr, n2 * 8, cudaMemcpyDeviceToHost, s);
-      if (ce == cudaSuccess) ce = cudaMemcpyAsync(Kh.data(), acc.ptr + n2, n2 * 8, cudaMemcpyDeviceToHost, s);
-      if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-      if (ce != cudaSuccess) return DSS_ERR_CUDA;
-      E2 = 0.5 * (trace_sym_acc(Dt, Ja, n) + trace_sym_acc(Dt, Jh, n)) -
-           0.5 * (trace_sym_acc(Ds[0], Ka, n) + trace_sym_acc(Ds[1], Kh, n));
-    }
-    *E = trace_dense_packed(Dt, Hp, n) + E2 - trace_dense_packed(W, Sp, n) +
-         dss_nuclear_repulsion(natom, Z, xyz.data());
+    if (ce != cudaSuccess) return dss_fail(ctx, DSS_ERR_CUDA, std::string("dss_gradient: ") + cudaGetErrorString(ce));
+    *E = trace_dense_packed(Dt, Hp, n) - trace_dense_packed(W, Sp, n) + dss_nuclear_repulsion(natom, Z, xyz.data());
     xyz[3 * a + d] = xyz_bohr[3 * a + d];
     return DSS_OK;
   };
   for (int a = 0; a < natom; ++a)
     for (int d = 0; d < 3; ++d) {
       double Ep = 0.0, Em = 0.0;
-      rc = energy(a, d, step, &Ep);
-      if (rc == DSS_OK) rc = energy(a, d, -step, &Em);
-      if (rc != DSS_OK) return dss_fail(ctx, rc, std::string("dss_gradient: displaced point failed: ") + g->err);
-      grad[3 * a + d] = (Ep - Em) / (2.0 * step);
+      rc = energy1(a, d, step, &Ep);
+      if (rc == DSS_OK) rc = energy1(a, d, -step, &Em);
+      if (rc != DSS_OK) return rc;
+      grad[3 * a + d] = (Ep - Em) / (2.0 * step) + g2[3 * a + d];
     }
   return DSS_OK;
 }

@@ -149,6 +149,19 @@ class FockBuilder:
                                               ctypes.c_void_p(K_ptr), ms))
         return [float(v) for v in ms]
 
+    def time_build(self, D_ptr: int, J_ptr: int, K_ptr: int) -> float:
+        """Device milliseconds of one whole J/K build in the current launch shape."""
+        ms = ctypes.c_float()
+        self._check(self._L.dss_time_build(self._h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(J_ptr),
+                                           ctypes.c_void_p(K_ptr), ctypes.byref(ms)))
+        return float(ms.value)
+
+    def set_persistent(self, on: bool) -> None:
+        self._check(self._L.dss_set_persistent(self._h, 1 if on else 0))
+
+    def persistent(self) -> bool:
+        return bool(self._L.dss_get_persistent(self._h))
+
     def fp64_peak_tflops(self) -> float:
         t = ctypes.c_double()
         self._check(self._L.dss_probe_fp64_peak(self._h, ctypes.byref(t)))
@@ -246,6 +259,19 @@ class FockBuilder:
         xyz = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
         g = np.zeros(3 * sh.natom)
         self._check(self._L.dss_gradient(self._h, sh.natom, _ip(Z), _dp(xyz), float(step), _dp(g)))
+        return g.reshape(sh.natom, 3)
+
+    def eri_gradient(self, sh: ShellArrays, D: np.ndarray, Da: Optional[np.ndarray] = None,
+                     Db: Optional[np.ndarray] = None) -> np.ndarray:
+        """Analytic four-centre gradient term [natom, 3] of packed-U densities
+        (D total; Da, Db spin densities of an unrestricted determinant)."""
+        atom = np.ascontiguousarray(sh.shell_atom, dtype=np.int32)
+        g = np.zeros(3 * sh.natom)
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        pa = np.ascontiguousarray(Da, dtype=np.float64) if Da is not None else None
+        pb = np.ascontiguousarray(Db, dtype=np.float64) if Db is not None else None
+        self._check(self._L.dss_eri_gradient(self._h, _dp(D), _dp(pa) if pa is not None else None,
+                                             _dp(pb) if pb is not None else None, sh.natom, _ip(atom), _dp(g)))
         return g.reshape(sh.natom, 3)
 
     def sync(self) -> None:

@@ -16,8 +16,10 @@
 //       for J, scf::density_matrix[spin] for K) and then serves elements from
 //       the cached matrices.  For RHF the exchange of D_alpha is K[D_total]/2,
 //       so one build per Fock matrix serves both sweeps.
-//   addExactTwoElectronGradient(v)  (:125-195): not provided by the engine; the
-//       shim reports that on stderr and leaves v unchanged.
+//   addExactTwoElectronGradient(v)  (:125-195): adds the analytic four-centre
+//       term of dss_eri_gradient (derivative ERIs digested with the two-particle
+//       density of scf::total_density_matrix and, for UHF, density_matrix[0/1])
+//       to v, with the nucleus of each shell from scf::basis_atoms.
 //
 // Errors follow the reference's convention (lalib/Lapack.cpp:33-38): a message
 // on stderr and the run continues; the affected matrix elements read as NaN.
@@ -38,6 +40,7 @@ int g_n = 0;
 std::vector<double> g_J, g_K[2];  // packed-U caches
 bool g_k_from_total = false;      // g_K[0] holds K[D_total]/2 from the last Coulomb build
 std::vector<double> g_Dp, g_Jtmp, g_Ktmp;
+std::vector<int> g_shell_f0;  // first basis function of each shell
 
 const double kNaN = std::numeric_limits<double>::quiet_NaN();
 
@@ -85,10 +88,12 @@ void assignExactRepulsionTensor() {
   // scf::basis holds 2l+1 consecutive functions per shell (SCFBasis.cpp:129-136).
   std::vector<int> l, nprim;
   std::vector<double> exps, coefs, centers;
+  g_shell_f0.clear();
   for (size_t f = 0; f < basis.size();) {
     const flo::ContractedGaussian& g = basis[f];
     size_t e = f + 1;
     while (e < basis.size() && e - f < 2 * g.l + 1 && same_shell(basis[e], g)) ++e;
+    g_shell_f0.push_back((int)f);
     l.push_back((int)g.l);
     nprim.push_back((int)g.primitives.size());
     for (const flo::GTOPrimitive& p : g.primitives) {
@@ -157,8 +162,27 @@ double getExactExchangeMatrix(uint mu, uint nu, Spin spin) {
 }
 
 void addExactTwoElectronGradient(VectorNd& target) {
-  (void)target;
-  std::cerr << "ERROR (GPU Fock build): two-electron gradients are not provided by the GPU engine\n";
+  if (!g_ctx || !g_n) return;
+  const int natom = (int)(target.size() / 3);
+  std::vector<int> shell_atom(g_shell_f0.size());
+  for (size_t q = 0; q < g_shell_f0.size(); ++q) shell_atom[q] = (int)basis_atoms[g_shell_f0[q]];
+  pack_density(total_density_matrix);
+  const std::vector<double> Dt = g_Dp;
+  std::vector<double> Da, Db;
+  if (spin_treatment == SpinTreatment::unrestricted) {
+    pack_density(density_matrix[0]);
+    Da = g_Dp;
+    pack_density(density_matrix[1]);
+    Db = g_Dp;
+  }
+  std::vector<double> g(3 * (size_t)natom, 0.0);
+  if (dss_eri_gradient(g_ctx, Dt.data(), Da.empty() ? nullptr : Da.data(), Db.empty() ? nullptr : Db.data(), natom,
+                       shell_atom.data(), g.data()) != DSS_OK) {
+    report("dss_eri_gradient");
+    for (size_t i = 0; i < g.size(); ++i) target[i] = kNaN;
+    return;
+  }
+  for (size_t i = 0; i < g.size(); ++i) target[i] += g[i];
 }
 
 }  // namespace scf

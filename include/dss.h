@@ -137,7 +137,11 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* shell_quartets
  * 2 and 3 one thread per shell quartet with one and two fewer resident blocks
  * per SM and so more registers per thread (classes of total angular momentum
  * <= 4; the plain FP64 reference-Boys build, other forms run variant 0's
- * kernel), -1 the library default.  Used by the autotuner; persists across bases. */
+ * kernel), 4 one thread per shell quartet in persistent blocks that stage the
+ * reference-mode Boys records of the class's orders in shared memory (classes
+ * of total angular momentum <= 2; the plain FP64 reference-Boys build of an
+ * unsplit launch, otherwise variant 0's kernel), -1 the library default.  Used
+ * by the autotuner; persists across bases. */
 int dss_set_class_variant(dss_ctx* ctx, int i, int variant);
 
 /* The variant class i currently runs with (-1 before a basis is set). */
@@ -151,6 +155,22 @@ int dss_kernels_per_build(const dss_ctx* ctx);
  * classes without work).  Synchronises the stream. */
 int dss_profile_build(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev,
                       float* ms_per_class);
+
+/* Persistent grouped launches (on = 1; 0 restores one launch per class, the
+ * default): the unsplit thread-per-quartet classes of total angular momentum
+ * <= 2, and those of 3..4, each share one persistent kernel whose warps take
+ * warp tasks of every class of the group from a device work queue (an atomic
+ * head, zeroed before each launch); warp-cooperative, split and heavier
+ * classes keep their own launches.  Plain FP64 reference-Boys builds and the
+ * mixed-precision form; other builds run per class.  No counterpart in the
+ * reference; chosen by the autotuner (dss_time_build). */
+int dss_set_persistent(dss_ctx* ctx, int on);
+int dss_get_persistent(const dss_ctx* ctx);
+
+/* One dss_build_jk_device (every class, in the launch shape the context is set
+ * to) timed with one CUDA event pair; *ms receives its device time.
+ * Synchronises the stream. */
+int dss_time_build(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev, float* ms);
 
 /* Device Boys function F_0..F_L (L <= 12) at n points x[] into F[n*(L+1)]:
  * mode DSS_BOYS_REF (the reference's truncated series, evaluated from the
@@ -263,13 +283,25 @@ int dss_load_density(dss_ctx* ctx, const char* path, int nbf, int* spins, int* n
 
 /* Nuclear gradient dE/dR (grad[3*natom], hartree/bohr) of the last
  * dss_scf_solve / dss_uhf_solve, the quantity of scf::getEnergyGradient
- * (chem/scf/Gradient.cpp:14-133, chem/scf/ExactCoulomb.cpp:125-195): the
- * fixed-density energy tr(D H) + E_2e[D] - tr(W S) + V_nn (W the energy-weighted
- * density of the final orbitals) differentiated by central differences of
- * step bohr (1e-4 is a good choice) along each nuclear coordinate, each point a
- * device one-electron evaluation and a device J/K build on displaced shells.
- * Not an analytic derivative: O(step^2) truncation, 6 natom builds. */
+ * (chem/scf/Gradient.cpp:14-133, chem/scf/ExactCoulomb.cpp:125-195):
+ * tr(D dH) + 1/2 sum Gamma d(ij|kl) - tr(W dS) + dV_nn, W the energy-weighted
+ * density of the final orbitals.  The two-electron term is analytic (as
+ * dss_eri_gradient); the one-electron terms are central differences of step
+ * bohr (1e-4 is a good choice) of the device one-electron integrals at fixed D
+ * and W (O(step^2) truncation, 6 natom one-electron evaluations, no J/K build). */
 int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double* xyz_bohr, double step, double* grad);
+
+/* Analytic four-centre term of the nuclear gradient, added into grad[3*natom]:
+ * 1/2 sum_{ijkl} Gamma_ijkl d(ij|kl)/dR with Gamma_ijkl = D_ij D_kl -
+ * sum_s D^s_ik D^s_jl, over the Schwarz-screened quartets of the current basis
+ * (derivative integrals from the 2 zeta-weighted shifted classes, digested with
+ * the two-particle density on the device).  Replaces addExactTwoElectronGradient
+ * (chem/scf/ExactCoulomb.cpp:125-195).  D_packed: total density; Da_packed and
+ * Db_packed: the spin densities for an unrestricted determinant, both NULL for a
+ * closed shell (D^s = D/2).  shell_atom[s]: the nucleus (0..natom-1) of shell s.
+ * Packed-U host arrays; single-molecule contexts. */
+int dss_eri_gradient(dss_ctx* ctx, const double* D_packed, const double* Da_packed, const double* Db_packed,
+                     int natom, const int* shell_atom, double* grad);
 
 /* ---------------------------------------------------------------- batches of molecules */
 /* Many closed-shell molecules of uneven size solved together: each ERI class
@@ -322,6 +354,13 @@ int dss_batch_finished(const dss_batch* batch, int* handles, int cap, int* count
  * ms[i] = milliseconds of class i in dss_class_info order, 0 for classes without
  * work.  Overwrites the molecules' J/K scratch only; for the batch autotuner. */
 int dss_batch_profile(dss_batch* batch, float* ms);
+
+/* One FP64 J/K accumulation over every live molecule in the batch's launch
+ * shape (per class, or persistent groups), timed as a whole: *ms. */
+int dss_batch_time_build(dss_batch* batch, float* ms);
+
+/* dss_set_persistent for the batch's builds (the captured iteration is re-made). */
+int dss_batch_set_persistent(dss_batch* batch, int on);
 
 /* Releases a molecule's region. */
 int dss_batch_remove(dss_batch* batch, int handle);

@@ -124,3 +124,21 @@ def test_batch_finished_poll_profile_and_tuner():
             E, _, it, st = b.result(h)
             assert st == 0
             assert abs(E - float(d["E"])) < 1e-9
+
+
+def test_batch_persistent_launch_same_energies():
+    # Persistent grouped launches (the L <= 2 and L = 3..4 thread-per-quartet
+    # classes each in one kernel fed by a device work queue): the reference's
+    # energies in the plain form, and the mixed form within 1 uEh of them.
+    cases = [load_case(n) for n in MIX]
+    for mixed, tol in ((False, 1e-9), (True, 1e-6)):
+        with Batch(schwarz_threshold=0.0, boys_mode=BOYS_REF) as b:
+            b.set_persistent(True)
+            hs = [b.add(sh) for (_, _, sh) in cases]
+            b.solve(conv=1e-10, mixed=mixed)
+            for (d, _, _), h in zip(cases, hs):
+                E, _, it, st = b.result(h)
+                assert st == 0
+                assert abs(E - float(d["E"])) < tol, (mixed, E, float(d["E"]))
+            t = b.time_build()
+            assert t > 0.0

@@ -100,7 +100,7 @@ def test_kernel_variants_agree(builders, name):
     fb.set_basis(sh)
     n = fb.num_classes()
     results = []
-    for variant in (0, 2, 3, 1):
+    for variant in (0, 2, 3, 1, 4):
         for i in range(n):
             try:
                 fb.set_class_variant(i, variant)
@@ -112,3 +112,20 @@ def test_kernel_variants_agree(builders, name):
         results.append((J, K))
     for i in range(n):
         fb.set_class_variant(i, -1)
+
+
+@pytest.mark.parametrize("name", ["dimer_631gs", "dimer_631gs_6d", "water_sto3g"])
+def test_persistent_launch_matches_reference(builders, name):
+    # The grouped persistent kernels (device work queue over the classes of a
+    # register group) reproduce the reference's J and K like the per-class launches.
+    d, mol, sh = load_case(name)
+    fb = builders[BOYS_REF]
+    fb.set_basis(sh)
+    fb.set_persistent(True)
+    try:
+        for _ in range(2):  # the queue heads are re-zeroed before every launch
+            J, K = fb.jk(2.0 * d["D_rand"])
+            assert np.abs(J - d["J_rand"]).max() < 1e-10
+            assert np.abs(0.5 * K - d["K_rand"]).max() < 1e-10
+    finally:
+        fb.set_persistent(False)
