@@ -415,9 +415,9 @@ def run_gpu(args):
     # tiers or warp-cooperative, the fastest by per-launch events.
     from dollarstorescf_b200 import autotune
 
-    variants = autotune.tune(fb, Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
+    variants = autotune.tune(fb, Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr(), cache_path=args.tune_cache)
     # Launch shape of the whole build: one launch per class or persistent grouped launches.
-    launch_shape = autotune.tune_launch(fb, Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr())
+    launch_shape = autotune.tune_launch(fb, Dd.data_ptr(), Jd.data_ptr(), Kd.data_ptr(), cache_path=args.tune_cache)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -720,6 +720,9 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the SCF / batch / serving measurements")
     ap.add_argument("--forms-molecules", type=int, default=256, help="alkanes in the batched-form measurement")
     ap.add_argument("--forms-requests", type=int, default=200, help="requests in the serving measurement")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON file of autotuner choices: reused when present, written when not (a profiler run "
+                         "then repeats the plain run's choices instead of re-timing them under serialisation)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -85,9 +85,21 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
     return choice
 
 
-def tune_launch(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 3) -> Dict[str, object]:
+def tune_launch(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 3,
+                cache_path: Optional[str] = None, key_extra: str = "") -> Dict[str, object]:
     """Per-class launches or persistent grouped launches for the whole build,
-    whichever times faster (best of `repeats` whole builds each)."""
+    whichever times faster (best of `repeats` whole builds each).  With
+    cache_path, a choice stored for the same key (the work's size bucket) is
+    reused instead of timed."""
+    cache = {}
+    if cache_path and os.path.isfile(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    sq, _, _ = fb.work_stats()
+    key = f"launch|{key_extra}|q{int(math.log2(max(1, sq)))}"
+    if key in cache:
+        fb.set_persistent(bool(cache[key]["persistent"]))
+        return dict(cache[key], cached=True)
     t = {}
     for on in (False, True):
         fb.set_persistent(on)
@@ -95,7 +107,12 @@ def tune_launch(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: in
         t[on] = min(fb.time_build(D_ptr, J_ptr, K_ptr) for _ in range(repeats))
     best = min(t, key=t.get)
     fb.set_persistent(best)
-    return {"persistent": best, "ms_per_class_launches": t[False], "ms_persistent": t[True]}
+    out = {"persistent": best, "ms_per_class_launches": t[False], "ms_persistent": t[True]}
+    if cache_path:
+        cache[key] = out
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    return out
 
 
 def tune_batch_launch(batch, repeats: int = 3) -> Dict[str, object]:

@@ -327,7 +327,7 @@ __device__ __forceinline__ void boys_ref_walk(double x, double* F) {
 // breakpoint b the cell may contain (b = 1e300 when it has none) and b itself;
 // a second record at the same index of block B holds the piece past b.
 // Orders with x > 1.1 m + 25 take the asymptotic form (one rsqrt for all of
-// them); every other order reads its A record (four 16-byte loads, b included),
+// them); every other order reads its A record (two 32-byte loads, b included),
 // the B record only when x > b, and evaluates seven FMAs: no search.  The
 // series itself (a separate function) runs only for x < 1/32 (cell 0 holds
 // several breakpoints) and within 4e-14 (relative) of a breakpoint, where the
@@ -351,6 +351,12 @@ __device__ __forceinline__ void dss_boys_smem_stage(const double* __restrict__ c
 
 template <int L>
 __host__ __device__ constexpr size_t dss_boys_smem_bytes() { return (size_t)(L + 1) * DSS_BOYS_NCELL * 64; }
+
+// One 32-byte read-only load (four doubles, 32-byte aligned address): a cell
+// record takes two of them instead of four 16-byte loads.
+__device__ __forceinline__ void dss_ld4(const double* __restrict__ p, double& a, double& b, double& c, double& d) {
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
 
 template <int L, bool SMEM = false>
 __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double* __restrict__ cells) {
@@ -383,7 +389,7 @@ __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
     if (m < m_lo) continue;
-    const double2* r = reinterpret_cast<const double2*>(cells) + ((size_t)m * DSS_BOYS_NCELL + k) * 4;
+    const double* r = cells + ((size_t)m * DSS_BOYS_NCELL + k) * 8;
     double2 c01, c23, c45, c6b;
     if constexpr (SMEM) {
       const int rec = m * DSS_BOYS_NCELL + k;
@@ -392,18 +398,14 @@ __device__ __forceinline__ void boys_ref_cells(double x, double* F, const double
       c45 = dss_boys_smem[dss_boys_smem_slot(rec, 2)];
       c6b = dss_boys_smem[dss_boys_smem_slot(rec, 3)];
     } else {
-      c01 = __ldg(r);
-      c23 = __ldg(r + 1);
-      c45 = __ldg(r + 2);
-      c6b = __ldg(r + 3);
+      dss_ld4(r, c01.x, c01.y, c23.x, c23.y);
+      dss_ld4(r + 4, c45.x, c45.y, c6b.x, c6b.y);
     }
     const double b = c6b.y;
     if (x > b) {  // the piece past the cell's breakpoint, same index in block B
-      r += (size_t)DSS_BOYS_NMC * DSS_BOYS_NCELL * 4;
-      c01 = __ldg(r);
-      c23 = __ldg(r + 1);
-      c45 = __ldg(r + 2);
-      c6b = __ldg(r + 3);
+      r += (size_t)DSS_BOYS_NMC * DSS_BOYS_NCELL * 8;
+      dss_ld4(r, c01.x, c01.y, c23.x, c23.y);
+      dss_ld4(r + 4, c45.x, c45.y, c6b.x, c6b.y);
     }
     double f = c6b.x;
     f = f * dx + c45.y;

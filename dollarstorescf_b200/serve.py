@@ -173,7 +173,11 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
         if own:
             b.close()
     wall = time.perf_counter() - t0
+    return _summary(results, wall, peak_inflight, admissions_deferred, t_admit, step_changed, step_same)
 
+
+def _summary(results: List[Result], wall: float, peak_inflight: int, admissions_deferred: int, t_admit: float,
+             step_changed: List[float], step_same: List[float]) -> Dict:
     def pct(vals, q):
         return float(np.percentile(np.array(vals), q) * 1e3) if len(vals) else None
 
@@ -201,3 +205,118 @@ def serve(requests: List[Request], conv: float = 1e-10, max_iter: int = 128, boy
         "steps_unchanged": len(step_same),
         "step_unchanged_ms": float(np.mean(step_same) * 1e3) if step_same else None,
     }
+
+
+def serve_pipelined(requests: List[Request], pipelines: int = 2, conv: float = 1e-10, max_iter: int = 128,
+                    boys_mode: int = BOYS_REF, arena_bytes: int = 0, mixed: bool = False, **mixed_opts) -> Dict:
+    """The serving loop over `pipelines` batches, each with its own context and
+    stream, stepped by its own host thread (the library calls release the
+    interpreter lock).  One batch's eigensolver, DIIS and host-side rebuild
+    overlap another batch's ERI launches on the GPU.  Each arrived request goes
+    to the batch with the least work in flight (sum of n^2 over its molecules);
+    each batch admits by its own arena (arena_bytes per batch) and retires its
+    finished molecules after every step, as serve() does."""
+    import threading
+
+    batches = [Batch(schwarz_threshold=1e-12, boys_mode=boys_mode, arena_bytes=arena_bytes)
+               for _ in range(pipelines)]
+    pending = sorted(requests, key=lambda r: r.arrival)
+    lock = threading.Lock()
+    state = {"qi": 0, "peak": 0, "deferred": 0, "t_admit": 0.0}
+    queues: List[List[Request]] = [[] for _ in range(pipelines)]
+    load = [0] * pipelines
+    inflight_count = [0] * pipelines
+    results: List[Result] = []
+    step_changed: List[float] = []
+    step_same: List[float] = []
+    errors: List[BaseException] = []
+    t0 = time.perf_counter()
+
+    def dispatch(now: float) -> None:
+        # caller holds the lock
+        while state["qi"] < len(pending) and pending[state["qi"]].arrival <= now:
+            r = pending[state["qi"]]
+            state["qi"] += 1
+            k = min(range(pipelines), key=lambda j: load[j])
+            queues[k].append(r)
+            load[k] += r.shells.nbf() ** 2
+
+    def worker(k: int) -> None:
+        b = batches[k]
+        inflight: Dict[int, tuple] = {}
+        changed = True
+        try:
+            while True:
+                with lock:
+                    now = time.perf_counter() - t0
+                    dispatch(now)
+                    mine, queues[k] = queues[k], []
+                    finished_all = state["qi"] >= len(pending)
+                    next_arrival = pending[state["qi"]].arrival if state["qi"] < len(pending) else None
+                still = []
+                for r in mine:
+                    try:
+                        ta = time.perf_counter()
+                        h = b.add(r.shells, guess=r.guess)
+                        dt = time.perf_counter() - ta
+                        inflight[h] = (r, time.perf_counter() - t0)
+                        changed = True
+                        with lock:
+                            state["t_admit"] += dt
+                    except Exception as e:  # arena full: retry after a step frees regions
+                        if getattr(e, "code", None) == -2:
+                            still.append(r)
+                        else:
+                            raise
+                if still:
+                    with lock:
+                        state["deferred"] += len(still)
+                        queues[k] = still + queues[k]
+                with lock:
+                    inflight_count[k] = len(inflight)
+                    state["peak"] = max(state["peak"], sum(inflight_count))
+                if not inflight:
+                    with lock:
+                        empty = not queues[k]
+                    if finished_all and empty:
+                        return
+                    if next_arrival is not None:
+                        time.sleep(max(0.0, min(0.005, next_arrival - (time.perf_counter() - t0))))
+                    continue
+                ts = time.perf_counter()
+                b.step(1, conv=conv, max_iter=max_iter, mixed=mixed, **mixed_opts)
+                dt = time.perf_counter() - ts
+                out = []
+                freed = 0
+                for h in b.finished_handles():
+                    if h not in inflight:
+                        continue
+                    E, _, it, st = b.result(h)
+                    r, adm = inflight.pop(h)
+                    b.remove(h)
+                    freed += r.shells.nbf() ** 2
+                    out.append(Result(r.rid, r.kind, E, it, st, r.arrival, adm, time.perf_counter() - t0))
+                with lock:
+                    (step_changed if changed else step_same).append(dt)
+                    results.extend(out)
+                    load[k] -= freed
+                changed = bool(out)
+        except BaseException as e:  # surfaced to the caller after the join
+            with lock:
+                errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(pipelines)]
+    try:
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    finally:
+        for b in batches:
+            b.close()
+    if errors:
+        raise errors[0]
+    wall = time.perf_counter() - t0
+    out = _summary(results, wall, state["peak"], state["deferred"], state["t_admit"], step_changed, step_same)
+    out["pipelines"] = pipelines
+    return out

@@ -95,3 +95,21 @@ def test_admission_waits_for_memory_and_results_do_not_change():
     for req, res in zip(reqs, sorted(out["results"], key=lambda r: r.rid)):
         E, _, it, st = solo_energy(req.shells, req.guess)
         assert abs(res.energy - E) < 1e-9, (res.rid, res.energy, E)
+
+
+def test_pipelined_serving_results_equal_solo_results():
+    # Two batches, each with its own context, stream and host thread, overlap
+    # on the GPU: every request is still answered, each energy equals the same
+    # molecule solved alone, and both batches carried work.
+    dimer = geometry.water_dimer(3)
+    E0, D0 = serve.solve_parent(dimer)
+    reqs = serve.make_request_stream(count=24, rate=200.0, seed=11, parent_density=D0, dimer=dimer)
+    out = serve.serve_pipelined(reqs, pipelines=2, conv=1e-10)
+    assert out["solves"] == len(reqs) and out["converged"] == len(reqs)
+    assert out["pipelines"] == 2 and out["peak_inflight"] > 1
+    by_id = {r.rid: r for r in out["results"]}
+    assert sorted(by_id) == sorted(r.rid for r in reqs)
+    for req in reqs[:8]:
+        res = by_id[req.rid]
+        E, _, it, st = solo_energy(req.shells, req.guess)
+        assert abs(res.energy - E) < 1e-9, (req.kind, res.energy, E)
