@@ -227,6 +227,12 @@ int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* ex
 // One-electron S, T, V (packed-U, device buffers) of one molecule's basis,
 // computed on the device on stream s (synchronous).  V == NULL: T receives
 // T + V, the core Hamiltonian.
+// One-electron part of the nuclear gradient, analytic (synchronous): grad_host
+// [3 natom] = sum D dH/dR - sum W dS/dR for dense n x n device densities D, W
+// (Hellmann-Feynman term included; the nuclear repulsion is not).
+int dss_one_electron_gradient(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz_bohr,
+                              const int* shell_atom, const double* D_dev, const double* W_dev, double* grad_host,
+                              std::string* errp, OneEScratch* scratch = nullptr);
 int dss_one_electron_device(cudaStream_t s, const BasisHost& B, int natom, const int* Z, const double* xyz,
                             double* S, double* T, double* V, std::string* err, OneEScratch* scratch = nullptr);
 // The same into host packed-U arrays (any may be NULL), plus the nuclear repulsion.

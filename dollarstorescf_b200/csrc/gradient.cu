@@ -8,10 +8,12 @@
 // (RHF: twice the alpha sum) and the two-particle density of the converged
 // determinant.  The two-electron term is analytic: derivative ERIs fused with the
 // two-particle-density digest on the device (dss_eri_gradient_dense,
-// eri_gradient.cu).  The one-electron terms differentiate S, T and V at fixed D
-// and W by central differences of the device one-electron integrals (the basis
-// functions move with their nucleus; step h, truncation error O(h^2): h = 1e-4
-// bohr gives ~1e-9 Eh/bohr), 6 natom one-electron evaluations and no J/K build.
+// eri_gradient.cu).  The one-electron terms are analytic too
+// (dss_one_electron_gradient: shifted overlap, kinetic and nuclear-attraction
+// integrals contracted with D and W, Hellmann-Feynman term included), and the
+// nuclear repulsion's derivative is added on the host.  With step > 0 the
+// one-electron terms are instead central differences of step bohr of the device
+// one-electron integrals at fixed D and W (6 natom evaluations; a cross-check).
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -39,8 +41,8 @@ extern "C" int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double*
                             double* grad) {
   if (!ctx) return DSS_ERR_INVALID;
   ctx->err.clear();
-  if (natom <= 0 || !Z || !xyz_bohr || !grad || !(step > 0.0))
-    return dss_fail(ctx, DSS_ERR_INVALID, "dss_gradient: empty molecule, NULL array or step <= 0");
+  if (natom <= 0 || !Z || !xyz_bohr || !grad || !(step >= 0.0))
+    return dss_fail(ctx, DSS_ERR_INVALID, "dss_gradient: empty molecule, NULL array or negative step");
   if (ctx->last_spins == 0 || ctx->nmol > 0)
     return dss_fail(ctx, DSS_ERR_INVALID, "dss_gradient: no solved single molecule in this context");
   const BasisHost& B0 = ctx->basis;
@@ -95,6 +97,32 @@ extern "C" int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double*
   int rc = uhf ? dss_eri_gradient_dense(ctx, dDt, dDa, dDb, 0.5, natom, owner.data(), g2.data())
            : dss_eri_gradient_dense(ctx, dDt, dDt, nullptr, 0.25, natom, owner.data(), g2.data());
   if (rc != DSS_OK) return rc;
+  if (step == 0.0) {
+    // One-electron part analytic, nuclear repulsion on the host.
+    DevBuf<double> dW;
+    if (dW.resize(n2) != cudaSuccess) return dss_fail(ctx, DSS_ERR_OOM, "dss_gradient: device allocation failed");
+    e = cudaMemcpyAsync(dW.ptr, W.data(), n2 * 8, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return dss_fail(ctx, DSS_ERR_CUDA, std::string("dss_gradient: ") + cudaGetErrorString(e));
+    std::vector<double> g1(3 * (size_t)natom, 0.0);
+    std::string err;
+    rc = dss_one_electron_gradient(s, B0, natom, Z, xyz_bohr, owner.data(), dDt, dW.ptr, g1.data(), &err,
+                                   &ctx->oe_scratch);
+    if (rc != DSS_OK) return dss_fail(ctx, rc, "dss_gradient: " + err);
+    for (int a = 0; a < natom; ++a)
+      for (int d = 0; d < 3; ++d) {
+        // d/dR_a of sum_{b<c} Z_b Z_c / R_bc (chem/scf/Gradient.cpp:118-130)
+        double vn = 0.0;
+        for (int b = 0; b < natom; ++b) {
+          if (b == a) continue;
+          const double rx = xyz_bohr[3 * a] - xyz_bohr[3 * b], ry = xyz_bohr[3 * a + 1] - xyz_bohr[3 * b + 1],
+                       rz = xyz_bohr[3 * a + 2] - xyz_bohr[3 * b + 2];
+          const double r = std::sqrt(rx * rx + ry * ry + rz * rz);
+          vn -= (double)Z[a] * Z[b] * (xyz_bohr[3 * a + d] - xyz_bohr[3 * b + d]) / (r * r * r);
+        }
+        grad[3 * a + d] = g1[3 * a + d] + vn + g2[3 * a + d];
+      }
+    return DSS_OK;
+  }
   // One-electron part: E_1(R) = tr(D H(R)) - tr(W S(R)) + V_nn(R) at displaced nuclei.
   const size_t np = (size_t)n * (n + 1) / 2;
   std::vector<double> Sp(np), Hp(np);

@@ -253,8 +253,10 @@ class FockBuilder:
         checkpoint for the current basis; usable as scf()/uhf() guesses."""
         return load_density(path, self.nbf, self)
 
-    def gradient(self, sh: ShellArrays, step: float = 1e-4) -> np.ndarray:
-        """Nuclear gradient [natom, 3] (hartree/bohr) of the last scf()/uhf()."""
+    def gradient(self, sh: ShellArrays, step: float = 0.0) -> np.ndarray:
+        """Nuclear gradient [natom, 3] (hartree/bohr) of the last scf()/uhf():
+        analytic (step 0), or with the one-electron terms as central differences
+        of that step (bohr)."""
         Z = np.ascontiguousarray(sh.Z, dtype=np.int32)
         xyz = np.ascontiguousarray(sh.atom_xyz, dtype=np.float64).ravel()
         g = np.zeros(3 * sh.natom)

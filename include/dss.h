@@ -285,10 +285,11 @@ int dss_load_density(dss_ctx* ctx, const char* path, int nbf, int* spins, int* n
  * dss_scf_solve / dss_uhf_solve, the quantity of scf::getEnergyGradient
  * (chem/scf/Gradient.cpp:14-133, chem/scf/ExactCoulomb.cpp:125-195):
  * tr(D dH) + 1/2 sum Gamma d(ij|kl) - tr(W dS) + dV_nn, W the energy-weighted
- * density of the final orbitals.  The two-electron term is analytic (as
- * dss_eri_gradient); the one-electron terms are central differences of step
- * bohr (1e-4 is a good choice) of the device one-electron integrals at fixed D
- * and W (O(step^2) truncation, 6 natom one-electron evaluations, no J/K build). */
+ * density of the final orbitals.  step = 0: every term analytic on the device
+ * (the four-centre term as dss_eri_gradient; shifted overlap, kinetic and
+ * nuclear-attraction integrals with the Hellmann-Feynman term).  step > 0: the
+ * one-electron terms instead by central differences of step bohr of the device
+ * one-electron integrals at fixed D and W (a cross-check; O(step^2)). */
 int dss_gradient(dss_ctx* ctx, int natom, const int* Z, const double* xyz_bohr, double step, double* grad);
 
 /* Analytic four-centre term of the nuclear gradient, added into grad[3*natom]:

@@ -82,3 +82,18 @@ def test_gradient_needs_a_solve(fb):
         fresh.set_basis(sh)
         with pytest.raises(_lib.DssError):
             fresh.gradient(sh)
+
+
+@pytest.mark.parametrize("name", ["water_631gs", "water_631gs_6d", "ch4_631g"])
+def test_analytic_one_electron_terms_equal_difference_quotients(fb, name):
+    # step 0: overlap, kinetic and nuclear-attraction derivatives analytic
+    # (Hellmann-Feynman term included); step 1e-4: the same terms as central
+    # differences of the device one-electron integrals.  O(h^2) ~ 1e-9.
+    d, mol, sh = load_case(name)
+    fb.set_basis(sh)
+    E, D, it, rc = fb.scf(d["H"], d["S"], sh.n_electrons() // 2, float(d["e_nuc"]), conv=1e-10)
+    assert rc == 0
+    ga = fb.gradient(sh, step=0.0)
+    gf = fb.gradient(sh, step=1e-4)
+    assert np.abs(ga - gf).max() < 1e-7, np.abs(ga - gf).max()
+    assert np.abs(ga.sum(axis=0)).max() < 1e-9
