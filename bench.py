@@ -552,6 +552,9 @@ def run_gpu(args):
         "eri_shell_quartets_per_s": sq * value / ws, "eri_prim_quartets_per_s": pq * value / ws,
         "work": {"shell_quartets": sq, "prim_quartets": pq, "warp_tasks": wt},
         "per_class_ms": {c["class"]: round(t, 4) for c, t in zip(fl, per_class_ms) if t > 0},
+        # Algorithmic TFLOP/s of each class launch (its work / its event-timed duration).
+        "per_class_tflops": {c["class"]: round(c["flops"] / (t * 1e-3) / 1e12, 3)
+                             for c, t in zip(fl, per_class_ms) if t > 0},
         "clocks": clk.summary(), "wall_s": wall,
     }
     if rank == 0 and not args.no_cpu_baseline:
