@@ -552,6 +552,9 @@ def run_gpu(args):
         "eri_shell_quartets_per_s": sq * value / ws, "eri_prim_quartets_per_s": pq * value / ws,
         "work": {"shell_quartets": sq, "prim_quartets": pq, "warp_tasks": wt},
         "per_class_ms": {c["class"]: round(t, 4) for c, t in zip(fl, per_class_ms) if t > 0},
+        # Screened shell quartets, primitive quartets and warp tasks of each class.
+        "per_class_work": {c["class"]: [c["shell_quartets"], c["prim_quartets"], c["warp_tasks"]]
+                           for c in fl if c["shell_quartets"]},
         # Algorithmic TFLOP/s of each class launch (its work / its event-timed duration).
         "per_class_tflops": {c["class"]: round(c["flops"] / (t * 1e-3) / 1e12, 3)
                              for c, t in zip(fl, per_class_ms) if t > 0},
@@ -683,7 +686,9 @@ def measure_forms(device: int, n_alkanes: int, n_requests: int):
             "plain_sequential": solve_plain([r.shells for r in reqs], [r.guess for r in reqs], max_iter=64)}
     served = {}
     for name, mixed in (("served_fp64", False), ("served_mixed", True)):
-        sv = serve.serve(reqs, conv=1e-10, boys_mode=BOYS_REF, mixed=mixed, max_iter=64)
+        # Three SCF iterations per batch step (one graph replay each) between
+        # admissions and retirements: fewer host round trips and pair-list rebuilds.
+        sv = serve.serve(reqs, conv=1e-10, boys_mode=BOYS_REF, mixed=mixed, max_iter=64, iterations_per_step=3)
         served[name] = {r.rid: (r.energy, r.status) for r in sv["results"]}
         sres[name] = {k: v for k, v in sv.items() if k != "results"}
     pairs = [(served["served_fp64"][k][0], v[0]) for k, v in served["served_mixed"].items()
@@ -698,7 +703,8 @@ def measure_forms(device: int, n_alkanes: int, n_requests: int):
     with Batch(device=device, schwarz_threshold=1e-12, boys_mode=BOYS_REF) as probe:
         need = sum(probe.info(n_for_region=r.shells.nbf())[2] for r in reqs)
     arena = max(need // 4, 1)
-    sv = serve.serve(reqs, conv=1e-10, boys_mode=BOYS_REF, mixed=True, max_iter=64, arena_bytes=arena)
+    sv = serve.serve(reqs, conv=1e-10, boys_mode=BOYS_REF, mixed=True, max_iter=64, arena_bytes=arena,
+                     iterations_per_step=3)
     sres["served_mixed_memory_bound"] = dict({k: v for k, v in sv.items() if k != "results"}, arena_bytes=arena)
     # At 200 req/s the queue grows for the whole stream, so p50/p99 above are
     # mostly queueing time (queue_p50 / service_p50 split them).  The same request
