@@ -22,7 +22,9 @@ warps pull warp tasks of every class of the group from a device queue), by
 timing whole builds (dss_time_build / dss_batch_time_build).
 
 Timing is per launch with CUDA events (dss_profile_build / dss_batch_profile
-run the classes one after another on one stream), best of `repeats`.  The best
+run the classes one after another on one stream), best of `repeats`; the
+choice is then refined on whole builds (refine_whole), where the classes run
+concurrently as they do in production.  The best
 shape depends on the class and on its quartet count, so the choice is redone
 per basis and can be cached by (class, pure, boys mode, quartet-count bucket).
 """
@@ -83,6 +85,95 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
     return choice
+
+
+def _median_of(f, k: int) -> float:
+    f()
+    ts = sorted(f() for _ in range(k))
+    return ts[k // 2]
+
+
+def refine_whole(time_build, set_variant, classes, choice: Dict[str, int], repeats: int = 5,
+                 passes: int = 1) -> Dict[str, object]:
+    """Coordinate descent of the per-class shapes on the time of whole builds.
+
+    The per-class timings run the classes one after another, but a build runs
+    them concurrently on side streams, where a shape that wins alone can lose:
+    the warp-cooperative kernels, for one, hold large shared-memory blocks that
+    crowd out the light classes running beside them.  Starting from the per-class
+    choice, every class (longest first) tries each of its shapes with the others
+    fixed and keeps the one whose whole build is fastest (median of `repeats`).
+    classes: [(index, name, [shapes])]."""
+    best = _median_of(time_build, repeats)
+    start = best
+    for _ in range(passes):
+        improved = False
+        for i, name, shapes in classes:
+            cur = choice[name]
+            for v in shapes:
+                if v == cur:
+                    continue
+                try:
+                    set_variant(i, v)
+                except Exception:
+                    continue
+                t = _median_of(time_build, repeats)
+                if t < best * 0.995:
+                    best, cur, improved = t, v, True
+            set_variant(i, cur)
+            choice[name] = cur
+        if not improved:
+            break
+    return {"ms_whole_build_per_class_choice": start, "ms_whole_build": best}
+
+
+def tune_whole(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, choice: Dict[str, int],
+               repeats: int = 5, cache_path: Optional[str] = None) -> Dict[str, object]:
+    """refine_whole for a single-molecule context (dss_time_build); updates
+    choice.  With cache_path, a refined choice stored for the same work size is
+    applied instead of re-timed."""
+    nc = fb.num_classes()
+    infos = [fb.class_info(i) for i in range(nc)]
+    names = ["%d%d%d%d" % tuple(info[0]) for info in infos]
+    cache = {}
+    if cache_path and os.path.isfile(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    sq, _, _ = fb.work_stats()
+    key = f"whole|q{int(math.log2(max(1, sq)))}"
+    if key in cache:
+        for i in range(nc):
+            if names[i] in cache[key]["choice"]:
+                fb.set_class_variant(i, int(cache[key]["choice"][names[i]]))
+                choice[names[i]] = int(cache[key]["choice"][names[i]])
+        return dict(cache[key]["result"], cached=True)
+    per = fb.profile_build(D_ptr, J_ptr, K_ptr)
+    order = sorted((i for i in range(nc) if infos[i][1] > 0 and names[i] in choice), key=lambda i: -per[i])
+    classes = [(i, names[i], VARIANTS) for i in order]
+    out = refine_whole(lambda: fb.time_build(D_ptr, J_ptr, K_ptr), fb.set_class_variant, classes, choice, repeats)
+    if cache_path:
+        cache[key] = {"choice": dict(choice), "result": out}
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    return out
+
+
+def tune_batch_whole(batch, choice: Dict[str, int], repeats: int = 3) -> Dict[str, object]:
+    """refine_whole for a dss_batch (dss_batch_time_build); updates choice."""
+    import ctypes
+
+    nc = batch._L.dss_num_classes()
+    ctx = batch._L.dss_batch_context(batch._h)
+    per = batch.profile()
+    names = {}
+    for i in range(nc):
+        l4 = (ctypes.c_int * 4)()
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        batch._L.dss_class_info(ctx, i, l4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        names[i] = "%d%d%d%d" % tuple(l4)
+    order = sorted((i for i in range(nc) if names[i] in choice and per[i] > 0), key=lambda i: -per[i])
+    classes = [(i, names[i], VARIANTS) for i in order]
+    return refine_whole(batch.time_build, batch.set_class_variant, classes, choice, repeats)
 
 
 def tune_launch(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 3,

@@ -64,6 +64,106 @@ __device__ __forceinline__ double coop_get(const double* __restrict__ rec, const
   return idx < 32u ? rec[idx] : vals[idx - 32u];
 }
 
+// The operations of one dependency level are independent, so a lane takes
+// several at a time: their records and all their operands are read before any
+// result is stored, which overlaps the dependent load chains.
+__device__ __forceinline__ void coop_vrr_fetch(const uint4& op, const double* __restrict__ r,
+                                               const double* __restrict__ vals, double (&x)[5]) {
+  const unsigned s0 = op.x >> 16, s1 = op.y & 0xFFFFu, s2 = op.y >> 16, s3 = op.z & 0xFFFFu, s4 = op.z >> 16;
+  x[0] = coop_get(r, vals, s0);
+  x[1] = coop_get(r, vals, s1);
+  x[2] = s2 != 0xFFFFu ? coop_get(r, vals, s2) : 0.0;
+  x[3] = s2 != 0xFFFFu ? coop_get(r, vals, s3) : 0.0;
+  x[4] = s4 != 0xFFFFu ? coop_get(r, vals, s4) : 0.0;
+}
+
+__device__ __forceinline__ double coop_vrr_value(const uint4& op, const double* __restrict__ r, const double (&x)[5]) {
+  const unsigned kind = op.w & 15u, ax = (op.w >> 4) & 3u;
+  const double k1 = (double)((op.w >> 8) & 0xFFu), k2 = (double)((op.w >> 16) & 0xFFu);
+  const bool has2 = (op.y >> 16) != 0xFFFFu, has4 = (op.z >> 16) != 0xFFFFu;
+  double v;
+  if (kind == 0u) {
+    v = r[12 + ax] * x[0] + r[15 + ax] * x[1];
+    if (has2) v += k1 * r[24] * (x[2] - r[27] * x[3]);
+  } else {
+    v = r[18 + ax] * x[0] + r[21 + ax] * x[1];
+    if (has2) v += k1 * r[25] * (x[2] - r[28] * x[3]);
+    if (has4) v += k2 * r[26] * x[4];
+  }
+  return v;
+}
+
+// One level of the VRR program over the primitive-quartet record r, four
+// operations per lane in flight (records and operands of all four read first).
+__device__ __forceinline__ void coop_vrr_level(const uint4* __restrict__ prog, int o0, int o1, int lane,
+                                               const double* __restrict__ r, double* vals) {
+  int o = o0 + lane;
+  for (; o + 96 < o1; o += 128) {
+    uint4 op[4];
+    double x[4][5];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) op[u] = __ldg(prog + o + 32 * u);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) coop_vrr_fetch(op[u], r, vals, x[u]);
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = coop_vrr_value(op[u], r, x[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) vals[(op[u].x & 0xFFFFu) - 32u] = v[u];
+  }
+  for (; o < o1; o += 32) {
+    const uint4 a = __ldg(prog + o);
+    double xa[5];
+    coop_vrr_fetch(a, r, vals, xa);
+    vals[(a.x & 0xFFFFu) - 32u] = coop_vrr_value(a, r, xa);
+  }
+}
+
+// HRR (kind 2) and function-transform (kind 3) operations over the value array.
+__device__ __forceinline__ void coop_hrr_fetch(const uint4& op, const double* __restrict__ vals, double (&x)[3]) {
+  const unsigned s0 = op.x >> 16, s1 = op.y & 0xFFFFu, s2 = op.y >> 16;
+  x[0] = vals[s0 - 32u];
+  x[1] = s1 != 0xFFFFu ? vals[s1 - 32u] : 0.0;
+  x[2] = s2 != 0xFFFFu ? vals[s2 - 32u] : 0.0;
+}
+
+__device__ __forceinline__ double coop_hrr_value(const uint4& op, const double* __restrict__ hdr,
+                                                 const double* __restrict__ wts, const double (&x)[3]) {
+  if ((op.w & 15u) == 2u) {
+    const unsigned ax = (op.w >> 4) & 3u, side = (op.w >> 6) & 1u;
+    return x[0] + hdr[3 * side + ax] * x[1];
+  }
+  double v = __ldg(wts + (op.z & 0xFFFFu)) * x[0];
+  if ((op.y & 0xFFFFu) != 0xFFFFu) v += __ldg(wts + (op.z >> 16)) * x[1];
+  if ((op.y >> 16) != 0xFFFFu) v += __ldg(wts + (op.w >> 16)) * x[2];
+  return v;
+}
+
+__device__ __forceinline__ void coop_hrr_level(const uint4* __restrict__ prog, int o0, int o1, int lane,
+                                               const double* __restrict__ hdr, const double* __restrict__ wts,
+                                               double* vals) {
+  int o = o0 + lane;
+  for (; o + 96 < o1; o += 128) {
+    uint4 op[4];
+    double x[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) op[u] = __ldg(prog + o + 32 * u);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) coop_hrr_fetch(op[u], vals, x[u]);
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = coop_hrr_value(op[u], hdr, wts, x[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) vals[(op[u].x & 0xFFFFu) - 32u] = v[u];
+  }
+  for (; o < o1; o += 32) {
+    const uint4 a = __ldg(prog + o);
+    double xa[3];
+    coop_hrr_fetch(a, vals, xa);
+    vals[(a.x & 0xFFFFu) - 32u] = coop_hrr_value(a, hdr, wts, xa);
+  }
+}
+
 template <int LA, int LB, int LC, int LD, bool PURE>
 __host__ __device__ constexpr size_t coop_smem_per_warp() {
   constexpr int NA = dss_nfunc(LA, PURE), NB = dss_nfunc(LB, PURE), NC = dss_nfunc(LC, PURE),
@@ -161,27 +261,25 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
       for (int j = 0; j < nb; ++j) {
         const double* __restrict__ r = recs + j * DSS_REC;
         for (int lv = 0; lv < P::NVLV; ++lv) {
-          const int o1 = __ldg(vlv + lv + 1);
-          for (int o = __ldg(vlv + lv) + lane; o < o1; o += 32) {
-            const uint4 op = __ldg(vrr + o);
-            const unsigned dst = op.x & 0xFFFFu, s0 = op.x >> 16, s1 = op.y & 0xFFFFu, s2 = op.y >> 16;
-            const unsigned s3 = op.z & 0xFFFFu, s4 = op.z >> 16;
-            const unsigned kind = op.w & 15u, ax = (op.w >> 4) & 3u;
-            const double k1 = (double)((op.w >> 8) & 0xFFu), k2 = (double)((op.w >> 16) & 0xFFu);
-            double v;
-            if (kind == 0u) {
-              v = r[12 + ax] * coop_get(r, vals, s0) + r[15 + ax] * coop_get(r, vals, s1);
-              if (s2 != 0xFFFFu) v += k1 * r[24] * (coop_get(r, vals, s2) - r[27] * coop_get(r, vals, s3));
-            } else {
-              v = r[18 + ax] * coop_get(r, vals, s0) + r[21 + ax] * coop_get(r, vals, s1);
-              if (s2 != 0xFFFFu) v += k1 * r[25] * (coop_get(r, vals, s2) - r[28] * coop_get(r, vals, s3));
-              if (s4 != 0xFFFFu) v += k2 * r[26] * coop_get(r, vals, s4);
-            }
-            vals[dst - 32u] = v;
-          }
+          coop_vrr_level(vrr, __ldg(vlv + lv), __ldg(vlv + lv + 1), lane, r, vals);
           __syncwarp();
         }
-        for (int o = lane; o < P::NACC; o += 32) {
+        // Accumulation: distinct targets, sources among the VRR outputs, four per lane in flight.
+        int o = lane;
+        for (; o + 96 < P::NACC; o += 128) {
+          unsigned dst[4];
+          double add[4], cur[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint4 op = __ldg(accp + o + 32 * u);
+            dst[u] = (op.x & 0xFFFFu) - 32u;
+            add[u] = coop_get(r, vals, op.x >> 16);
+            cur[u] = vals[dst[u]];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) vals[dst[u]] = cur[u] + add[u];
+        }
+        for (; o < P::NACC; o += 32) {
           const uint4 op = __ldg(accp + o);
           vals[(op.x & 0xFFFFu) - 32u] += coop_get(r, vals, op.x >> 16);
         }
@@ -190,22 +288,7 @@ __global__ void __launch_bounds__(32 * DSS_COOP_WARPS) eri_coop_kernel(EriArgs a
     }
     // HRR + transform
     for (int lv = 0; lv < P::NHLV; ++lv) {
-      const int o1 = __ldg(hlv + lv + 1);
-      for (int o = __ldg(hlv + lv) + lane; o < o1; o += 32) {
-        const uint4 op = __ldg(hrr + o);
-        const unsigned dst = op.x & 0xFFFFu, s0 = op.x >> 16, s1 = op.y & 0xFFFFu, s2 = op.y >> 16;
-        const unsigned kind = op.w & 15u;
-        double v;
-        if (kind == 2u) {
-          const unsigned ax = (op.w >> 4) & 3u, side = (op.w >> 6) & 1u;
-          v = vals[s0 - 32u] + hdr[3 * side + ax] * vals[s1 - 32u];
-        } else {
-          v = __ldg(wts + (op.z & 0xFFFFu)) * vals[s0 - 32u];
-          if (s1 != 0xFFFFu) v += __ldg(wts + (op.z >> 16)) * vals[s1 - 32u];
-          if (s2 != 0xFFFFu) v += __ldg(wts + (op.w >> 16)) * vals[s2 - 32u];
-        }
-        vals[dst - 32u] = v;
-      }
+      coop_hrr_level(hrr, __ldg(hlv + lv), __ldg(hlv + lv + 1), lane, hdr, wts, vals);
       __syncwarp();
     }
     // Digest (same algebra as eri_jk_kernel).

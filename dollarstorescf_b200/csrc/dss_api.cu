@@ -680,7 +680,7 @@ int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
     if ((size_t)idx < ctx->class_variant.size() && ctx->class_variant[idx] >= 0)
       ct.variant = ctx->class_variant[idx];
     else
-      ct.variant = dss_has_coop(ci.la, ci.lb, ci.lc, ci.ld) ? 1 : 0;
+      ct.variant = 0;  // thread per quartet; the tuner may pick other shapes
     ct.ntasks = (int)ht.tasks[idx].size();
     // A single molecule whose class has few warp tasks (a small molecule) would
     // leave most SMs idle while each lane walks its quartet's whole primitive
@@ -958,7 +958,7 @@ int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
   ctx->class_variant[i] = variant;
   if ((size_t)i < ctx->tasks.size()) {
     ClassTasks& ct = ctx->tasks[i];
-    ct.variant = variant >= 0 ? variant : (dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]) ? 1 : 0);
+    ct.variant = variant >= 0 ? variant : 0;
     if (ct.ntasks && ctx->nmol == 0 && cudaSetDevice(ctx->opts.device) == cudaSuccess)
       dss_preload_eri_variant(ct.la, ct.lb, ct.lc, ct.ld, ctx->opts.boys_mode, ctx->pure, ct.variant);
   }

@@ -140,7 +140,10 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* shell_quartets
  * kernel), 4 one thread per shell quartet in persistent blocks that stage the
  * reference-mode Boys records of the class's orders in shared memory (classes
  * of total angular momentum <= 2; the plain FP64 reference-Boys build of an
- * unsplit launch, otherwise variant 0's kernel), -1 the library default.  Used
+ * unsplit launch, otherwise variant 0's kernel), -1 the library default
+ * (variant 0: in a build the classes run concurrently, and the warp-cooperative
+ * kernels' large shared-memory blocks slow the classes beside them more than
+ * they gain, measured on the (H2O)16 6-31G* build 8.51 -> 7.21 ms).  Used
  * by the autotuner; persists across bases. */
 int dss_set_class_variant(dss_ctx* ctx, int i, int variant);
 
