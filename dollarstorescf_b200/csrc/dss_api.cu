@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -193,7 +194,12 @@ int dss_create(dss_ctx** out, const dss_opts* opts) {
   e = cudaSetDevice(ctx->opts.device);
   if (e == cudaSuccess) e = dss_boys_cell_table(&ctx->boys_cell);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
-  for (int i = 0; i < dss_ctx::kSideStreams && e == cudaSuccess; ++i) {
+  // Side streams the class launches of a build spread over (DSS_SIDE_STREAMS, 1..16).
+  if (const char* ns = std::getenv("DSS_SIDE_STREAMS")) {
+    const int v = std::atoi(ns);
+    if (v >= 1 && v <= dss_ctx::kSideStreams) ctx->nside = v;
+  }
+  for (int i = 0; i < ctx->nside && e == cudaSuccess; ++i) {
     e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev[i], cudaEventDisableTiming);
   }
@@ -776,7 +782,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   }
   if (fork) {
     DSS_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
-    for (int i = 0; i < dss_ctx::kSideStreams; ++i) DSS_CUDA(cudaStreamWaitEvent(ctx->side[i], ctx->fork_ev, 0));
+    for (int i = 0; i < ctx->nside; ++i) DSS_CUDA(cudaStreamWaitEvent(ctx->side[i], ctx->fork_ev, 0));
   }
   int slot = 0;
   auto common_args = [&](EriArgs& a) {
@@ -822,7 +828,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
       common_args(p.a);
       p.ncls = npg[g];
       p.head = ctx->d_persist_head.ptr + g;
-      cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
+      cudaStream_t st = fork ? ctx->side[slot++ % ctx->nside] : ctx->stream;
       DSS_CUDA(cudaMemsetAsync(p.head, 0, sizeof(int), st));
       if (!dss_launch_persist(g, eboys, ctx->pure, mode->mixed, p, st))
         return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_enqueue_jk: no persistent kernel for this form");
@@ -831,7 +837,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   }
   for (int ci : single) {
     ClassTasks& ct = ctx->tasks[ci];
-    cudaStream_t st = fork ? ctx->side[slot++ % dss_ctx::kSideStreams] : ctx->stream;
+    cudaStream_t st = fork ? ctx->side[slot++ % ctx->nside] : ctx->stream;
     EriArgs a{};
     common_args(a);
     a.tasks = ct.d_tasks.ptr;
@@ -844,7 +850,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     if (events) DSS_CUDA(cudaEventRecord(events[2 * ci + 1], st));
   }
   if (fork) {
-    for (int i = 0; i < dss_ctx::kSideStreams; ++i) {
+    for (int i = 0; i < ctx->nside; ++i) {
       DSS_CUDA(cudaEventRecord(ctx->join_ev[i], ctx->side[i]));
       DSS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join_ev[i], 0));
     }

@@ -90,7 +90,8 @@ struct dss_ctx {
   cudaStream_t own_stream = nullptr;  // created with the context
   // Side streams: the class launches of one build fork onto them so that the
   // long-running, low-occupancy high-angular-momentum classes overlap the rest.
-  static constexpr int kSideStreams = 6;
+  static constexpr int kSideStreams = 16;  // capacity; nside are used
+  int nside = 6;
   cudaStream_t side[kSideStreams] = {};
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[kSideStreams] = {};
