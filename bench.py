@@ -512,7 +512,8 @@ def run_gpu(args):
         with open(tpath) as f:
             for ln in f:
                 p = ln.split()
-                if len(p) == 2 and not ln.startswith("#") and p[0] == "eri_jk_kernel<%s>" % fl[dom]["class"]:
+                if len(p) == 2 and not ln.startswith("#") and \
+                        p[0] == "eri_jk_kernel<%s>/%s" % (fl[dom]["class"], variants.get(fl[dom]["class"], 0)):
                     traffic = int(p[1])
     kern = fb.kernels_per_build()
     hbm_peak = None

@@ -13,7 +13,10 @@ shape the library offers for it and keeps the fastest:
      compiled with it);
   4  one thread per shell quartet in persistent blocks of 8 warps that first
      stage the class's reference-mode Boys records (35 KB per order) in shared
-     memory, L <= 2.
+     memory, L <= 2;
+  5, 6, 7  shapes 0, 2, 3 on a one-wave grid (the blocks every SM holds at
+     once, the warps striding over the tasks): slower alone, but they leave
+     SMs to the classes launched beside them in a build.
 
 With the per-class shapes fixed, the launch shape of the whole build is chosen
 the same way: one launch per class, or persistent grouped launches (the
@@ -38,7 +41,7 @@ from typing import Dict, Optional
 from .engine import FockBuilder
 
 # Kernel shapes tried per class (see the module docstring).
-VARIANTS = (0, 2, 3, 1, 4)
+VARIANTS = (0, 2, 3, 1, 4, 5, 6, 7)
 
 
 def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,

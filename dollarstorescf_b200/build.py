@@ -63,9 +63,15 @@ def _class_tu(c, coop: bool) -> str:
     lines.append(f"void dss_launch_eri_jk_{name}(int boys, int pure, int mixed, int uhf, int tier, "
                  f"const EriArgs& a, cudaStream_t s) {{")
     tiers = la + lb + lc + ld <= 4  # dss_has_tiers
+    lines.append("  // tier 4..6: tiers 0..2 on a one-wave grid (the resident blocks of every SM; the")
+    lines.append("  // warps stride over the tasks), which leaves room for the classes launched beside it.")
+    lines.append("  const bool cap = tier >= 4;")
+    lines.append("  if (cap) tier -= 4;")
     lines.append("  const int threads = 128;")
-    lines.append("  const unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
+    lines.append("  unsigned blocks = (unsigned)(((long long)a.ntasks * 32 + threads - 1) / threads);")
     lines.append("  if (!blocks) return;")
+    lines.append(f"  if (cap) {{ const unsigned c = (unsigned)(dss_sm_count() * dss_min_blocks_tier({la + lb + lc + ld}, "
+                 f"tier)); if (blocks > c) blocks = c; }}")
     lines.append("  const dim3 grid(blocks, a.split > 1 ? (unsigned)a.split : 1u);")
     for boys, pure, mixed in combos:
         pb = "true" if pure else "false"
@@ -270,6 +276,7 @@ def _dispatch_tu(classes, pcls, coop) -> str:
     for (la, lb, lc, ld) in classes:
         lines.append(f"void dss_preload_eri_jk_{la}{lb}{lc}{ld}(int boys, int pure, int variant);")
     lines.append("void dss_preload_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant) {")
+    lines.append("  if (variant >= 5) variant = variant == 5 ? 0 : variant - 3;  // one-wave grids: same kernels")
     for (la, lb, lc, ld) in classes:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
                      f"return dss_preload_eri_jk_{la}{lb}{lc}{ld}(boys, pure, variant);")

@@ -948,7 +948,7 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* sq, long long*
 }
 
 int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
-  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 4) return DSS_ERR_INVALID;
+  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 7) return DSS_ERR_INVALID;
   if (ctx->class_variant.size() < (size_t)DSS_N_QUARTET_CLASSES) ctx->class_variant.assign(DSS_N_QUARTET_CLASSES, -1);
   static const int kL[][4] = {
 #define DSS_CLASS_L2(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_},
@@ -957,7 +957,8 @@ int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
   };
   if (variant == 1 && !dss_has_coop(kL[i][0], kL[i][1], kL[i][2], kL[i][3]))
     return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: no warp-cooperative kernel for this class");
-  if ((variant == 2 || variant == 3) && !dss_has_tiers(kL[i][0] + kL[i][1] + kL[i][2] + kL[i][3]))
+  if ((variant == 2 || variant == 3 || variant == 6 || variant == 7) &&
+      !dss_has_tiers(kL[i][0] + kL[i][1] + kL[i][2] + kL[i][3]))
     return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: this class has one register tier");
   if (variant == 4 && !dss_has_smem_variant(kL[i][0] + kL[i][1] + kL[i][2] + kL[i][3]))
     return dss_fail(ctx, DSS_ERR_UNSUPPORTED, "dss_set_class_variant: no shared-memory Boys shape for this class");

@@ -359,11 +359,27 @@ __device__ __forceinline__ void eri_jk_task(const EriArgs& a, const int4* __rest
 }
 
 // Thread per shell quartet, warp per task.  TIER: register tier (dss_min_blocks_tier).
+// The warps stride over the tasks, so a launch may use fewer blocks than tasks
+// (the one-wave grids of class variants 5-7).
 template <int LA, int LB, int LC, int LD, int BOYS, bool PURE, bool MIXED = false, bool UHF = false, int TIER = 0>
 __global__ void __launch_bounds__(128, dss_min_blocks_tier(LA + LB + LC + LD, TIER)) eri_jk_kernel(EriArgs a) {
-  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (warp >= a.ntasks) return;  // uniform per warp
-  eri_jk_task<LA, LB, LC, LD, BOYS, PURE, MIXED, UHF>(a, a.tasks, warp, threadIdx.x & 31, (int)blockIdx.y);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); warp < a.ntasks; warp += nwarps)
+    eri_jk_task<LA, LB, LC, LD, BOYS, PURE, MIXED, UHF>(a, a.tasks, warp, threadIdx.x & 31, (int)blockIdx.y);
+}
+
+// Multiprocessors of the current device (read once per device).
+inline int dss_sm_count() {
+  static std::atomic<int> cache[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int n = (dev >= 0 && dev < 64) ? cache[dev].load() : 0;
+  if (!n) {
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n < 1) n = 1;
+    if (dev >= 0 && dev < 64) cache[dev].store(n);
+  }
+  return n;
 }
 
 // The shared-memory Boys shape (class variant 4; plain form, reference Boys,
@@ -476,7 +492,8 @@ void dss_launch_schwarz(int la, int lb, int boys, int pure, const SchwarzArgs& a
 // variant 0: one thread per quartet; 1: warp-cooperative (when compiled for the class);
 // 2, 3: one thread per quartet in register tier 1, 2 (plain form: reference Boys,
 // FP64; other forms run tier 0); 4: the shared-memory Boys shape (plain form,
-// L <= 2; split launches and other forms run tier 0).  uhf = 1: the unrestricted variant (thread per
+// L <= 2; split launches and other forms run tier 0); 5, 6, 7: variants 0, 2, 3
+// on a one-wave grid.  uhf = 1: the unrestricted variant (thread per
 // quartet, reference Boys only).
 void dss_launch_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int mixed, int uhf, int variant,
                             const EriArgs& a, cudaStream_t s);
