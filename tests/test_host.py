@@ -167,3 +167,32 @@ def test_bench_replicas_take_the_slowest_rank_gloo():
         assert p.exitcode == 0
     assert [r[1] for r in res] == [2.0, 2.0]
     assert all(abs(r[2] - 10.0) < 1e-12 for r in res)
+
+
+def test_whole_build_refinement_finds_the_concurrent_optimum():
+    # refine_whole: coordinate descent over per-class shapes on a whole-build
+    # time.  A fake build whose time depends on the joint choice (class "a"
+    # is best with shape 1 only when "b" runs shape 0, as concurrency can make
+    # it) must end at the joint minimum, keep the starting shape of a class
+    # whose alternatives are rejected, and report both times.
+    from dollarstorescf_b200.autotune import refine_whole
+
+    state = {0: 0, 1: 5, 2: 0}
+
+    def set_variant(i, v):
+        if i == 2 and v != 0:
+            raise ValueError("shape not available for this class")
+        state[i] = v
+
+    def time_build():
+        t = 10.0
+        t -= 2.0 if (state[0] == 1 and state[1] == 0) else 0.0
+        t -= 1.0 if state[1] == 0 else 0.0
+        return t
+
+    choice = {"a": 0, "b": 5, "c": 0}
+    classes = [(1, "b", (0, 5)), (0, "a", (0, 1)), (2, "c", (0, 1))]
+    out = refine_whole(time_build, set_variant, classes, choice, repeats=1)
+    assert choice == {"a": 1, "b": 0, "c": 0}
+    assert state == {0: 1, 1: 0, 2: 0}
+    assert out["ms_whole_build_per_class_choice"] == 10.0 and out["ms_whole_build"] == 7.0
