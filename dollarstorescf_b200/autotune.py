@@ -57,7 +57,7 @@ def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,
     keys = [f"{names[i]}|{key_extra}|q{int(math.log2(max(1, infos[i][1])))}" for i in range(nc)]
     todo = [i for i in range(nc) if infos[i][1] > 0 and keys[i] not in cache]
     timings = {}
-    for variant in VARIANTS:
+    for variant in VARIANTS if todo else ():
         ok = []
         for i in todo:
             try:
