@@ -550,6 +550,13 @@ struct dss_batch_mol {
   PairSet pairs;    // its shell pairs and Schwarz factors, made once at admission
   bool needs_x = true;  // X = S^-1/2 not computed yet (done for all new molecules at the next step)
   long long pp_off = 0;  // its primitive pairs' first record in the batch's device pool
+  // Its work lists in the batch's device task pool: class i's tasks at
+  // task_off + task_cls_off[i], task_cnt[i] of them (pair indices local to the
+  // molecule; the host copies are dropped after the upload).
+  long long task_off = 0;
+  size_t task_n = 0;
+  std::vector<int> task_cnt;
+  std::vector<long long> task_cls_off;
 };
 
 // Device pool of the live molecules' primitive-pair records (10 doubles each),
@@ -565,6 +572,29 @@ struct PpPool {
   ~PpPool() {
     if (ptr) cudaFree(ptr);
   }
+};
+
+// Device pool of the live molecules' own work lists (int4 tasks), filled at
+// admission; a change of composition gathers the batch's lists from it on the
+// device (k_gather_tasks) instead of merging and uploading them from the host.
+// Removal leaves a hole; the pool is compacted when it grows.
+struct TaskPool {
+  int4* ptr = nullptr;
+  size_t cap = 0, used = 0;  // tasks
+  TaskPool() = default;
+  TaskPool(const TaskPool&) = delete;
+  TaskPool& operator=(const TaskPool&) = delete;
+  ~TaskPool() {
+    if (ptr) cudaFree(ptr);
+  }
+};
+
+// One run of a molecule's class-i tasks copied into the batch's class-i list,
+// its pair indices moved by (dx, dy) into the merged pair order, w = its slot.
+struct TaskSeg {
+  const int4* src;
+  int4* dst;
+  int n, dx, dy, slot;
 };
 
 struct dss_batch {
@@ -583,6 +613,9 @@ struct dss_batch {
   DevBuf<int> d_pending;  // per slot: 1 while the molecule's X is not computed
   DevBuf<double> admit_tmp;  // admission scratch (packed H, S, guess), grow-only
   PpPool pp_pool;
+  TaskPool task_pool;
+  DevBuf<TaskSeg> d_segs;       // the gather's segment table, grow-only
+  std::vector<TaskSeg> h_segs;  // its host image (kept until the next rebuild)
   int nmax = 0;
   int* h_nact = nullptr;  // pinned: molecules still iterating, molecules finished in the last iteration
   std::vector<int> last_finished;  // handles whose results the last dss_batch_step produced
@@ -683,6 +716,75 @@ int pool_put(dss_batch* b, dss_batch_mol* m) {
   return DSS_OK;
 }
 
+// Uploads a new molecule's work lists (all classes, one run) into the task
+// pool, growing and compacting it over the live molecules when full, and drops
+// the host copies.
+int task_put(dss_batch* b, dss_batch_mol* m) {
+  TaskPool& pool = b->task_pool;
+  cudaStream_t s = b->ctx->stream;
+  HostTasks& ht = m->pairs.tasks;
+  const size_t nq = ht.tasks.size();
+  m->task_cnt.assign(nq, 0);
+  m->task_cls_off.assign(nq, 0);
+  size_t rec = 0;
+  for (size_t ci = 0; ci < nq; ++ci) {
+    m->task_cls_off[ci] = (long long)rec;
+    m->task_cnt[ci] = (int)ht.tasks[ci].size();
+    rec += ht.tasks[ci].size();
+  }
+  if (pool.used + rec > pool.cap) {
+    size_t live = rec;
+    for (const auto& o : b->mols)
+      if (o.live) live += o.task_n;
+    const size_t cap = std::max<size_t>(std::max<size_t>(2 * pool.cap, live + live / 2), 1 << 16);
+    int4* np = nullptr;
+    if (cudaMalloc((void**)&np, cap * sizeof(int4)) != cudaSuccess) return DSS_ERR_OOM;
+    size_t at = 0;
+    for (auto& o : b->mols) {
+      if (!o.live) continue;
+      if (o.task_n && cudaMemcpyAsync(np + at, pool.ptr + o.task_off, o.task_n * sizeof(int4),
+                                      cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        cudaFree(np);
+        return DSS_ERR_CUDA;
+      }
+      o.task_off = (long long)at;
+      at += o.task_n;
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      cudaFree(np);
+      return DSS_ERR_CUDA;
+    }
+    if (pool.ptr) cudaFree(pool.ptr);
+    pool.ptr = np;
+    pool.cap = cap;
+    pool.used = at;
+    b->dirty = true;  // the live molecules' offsets moved
+  }
+  for (size_t ci = 0; ci < nq; ++ci) {
+    const std::vector<int4>& t = ht.tasks[ci];
+    if (!t.empty() && cudaMemcpyAsync(pool.ptr + pool.used + m->task_cls_off[ci], t.data(), t.size() * sizeof(int4),
+                                      cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return DSS_ERR_CUDA;
+  }
+  m->task_off = (long long)pool.used;
+  m->task_n = rec;
+  pool.used += rec;
+  // The copies above are from pageable memory, so they have left the host
+  // vectors when cudaMemcpyAsync returns.
+  for (auto& t : ht.tasks) std::vector<int4>().swap(t);
+  return DSS_OK;
+}
+
+__global__ void k_gather_tasks(const TaskSeg* __restrict__ segs, int nseg) {
+  for (int g = blockIdx.x; g < nseg; g += gridDim.x) {
+    const TaskSeg sg = segs[g];
+    for (int i = threadIdx.x; i < sg.n; i += blockDim.x) {
+      const int4 t = sg.src[i];
+      sg.dst[i] = make_int4(t.x + sg.dx, t.y + sg.dy, t.z, sg.slot);
+    }
+  }
+}
+
 // Rebuilds the batch basis (pairs, Schwarz factors, work lists) and the
 // per-slot tables for the live molecules.
 int rebuild(dss_batch* b) {
@@ -766,27 +868,49 @@ int rebuild(dss_batch* b) {
       acc += lc1[sl][c] - lc0[sl][c];
     }
   }
-  HostTasks merged;
-  const size_t nq = parts.empty() ? 0 : parts[0]->tasks.tasks.size();
-  merged.tasks.assign(nq, {});
-  merged.shell_quartets.assign(nq, 0);
-  merged.prim_quartets.assign(nq, 0);
+  const size_t nq = parts[0]->tasks.shell_quartets.size();
+  std::vector<int> cnt(nq, 0);
+  std::vector<long long> sq(nq, 0), pq(nq, 0);
+  for (size_t ci = 0; ci < nq; ++ci)
+    for (int sl = 0; sl < nb; ++sl) {
+      const dss_batch_mol& m = b->mols[b->slot_mol[sl]];
+      cnt[ci] += m.task_cnt[ci];
+      sq[ci] += parts[sl]->tasks.shell_quartets[ci];
+      pq[ci] += parts[sl]->tasks.prim_quartets[ci];
+    }
+  int rc = dss_pairs_install(ctx, std::move(B), std::move(P), nullptr, true);
+  if (rc != DSS_OK) return bfail(b, rc, ctx->err);
+  if ((rc = dss_install_task_counts(ctx, cnt, sq, pq)) != DSS_OK) return bfail(b, rc, ctx->err);
+  // The batch's lists, gathered on the device from the molecules' own lists in
+  // (class, slot) order.
+  b->h_segs.clear();
   for (size_t ci = 0; ci < nq; ++ci) {
     const int bc = dss_quartet_bra_class((int)ci), kc = dss_quartet_ket_class((int)ci);
-    size_t cnt = 0;
-    for (int sl = 0; sl < nb; ++sl) cnt += parts[sl]->tasks.tasks[ci].size();
-    std::vector<int4>& out = merged.tasks[ci];
-    out.reserve(cnt);
+    int at = 0;
     for (int sl = 0; sl < nb; ++sl) {
-      const HostTasks& ht = parts[sl]->tasks;
-      const int db = mc0[bc] + off[sl][bc] - lc0[sl][bc], dk = mc0[kc] + off[sl][kc] - lc0[sl][kc];
-      for (const int4& t : ht.tasks[ci]) out.push_back(make_int4(t.x + db, t.y + dk, t.z, sl));
-      merged.shell_quartets[ci] += ht.shell_quartets[ci];
-      merged.prim_quartets[ci] += ht.prim_quartets[ci];
+      const dss_batch_mol& m = b->mols[b->slot_mol[sl]];
+      const int n = m.task_cnt[ci];
+      if (!n) continue;
+      TaskSeg sg;
+      sg.src = b->task_pool.ptr + m.task_off + m.task_cls_off[ci];
+      sg.dst = ctx->tasks[ci].d_tasks.ptr + at;
+      sg.n = n;
+      sg.dx = mc0[bc] + off[sl][bc] - lc0[sl][bc];
+      sg.dy = mc0[kc] + off[sl][kc] - lc0[sl][kc];
+      sg.slot = sl;
+      b->h_segs.push_back(sg);
+      at += n;
     }
   }
-  int rc = dss_pairs_install(ctx, std::move(B), std::move(P), &merged);
-  if (rc != DSS_OK) return bfail(b, rc, ctx->err);
+  if (!b->h_segs.empty()) {
+    if (b->d_segs.resize(b->h_segs.size()) != cudaSuccess) return bfail(b, DSS_ERR_OOM, "batch: device tables");
+    if (cudaMemcpyAsync(b->d_segs.ptr, b->h_segs.data(), b->h_segs.size() * sizeof(TaskSeg), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess)
+      return bfail(b, DSS_ERR_CUDA, "batch: device tables");
+    const int nseg = (int)b->h_segs.size();
+    k_gather_tasks<<<(unsigned)std::min(nseg, 8192), 256, 0, ctx->stream>>>(b->d_segs.ptr, nseg);
+    if (cudaGetLastError() != cudaSuccess) return bfail(b, DSS_ERR_CUDA, "batch: task gather launch");
+  }
   ctx->nbf = 1;  // batch mode: accumulators are addressed per molecule
   if (ctx->d_dmax.resize((size_t)std::max<long long>(dtot, 1)) != cudaSuccess)
     return bfail(b, DSS_ERR_OOM, "batch: device tables");
@@ -1107,6 +1231,8 @@ int dss_batch_add(dss_batch* b, int n_shell, const int* l, const int* nprim, con
   if (rc != DSS_OK) return bfail(b, rc, std::string("dss_batch_add: shell pairs: ") + b->ctx->err);
   rc = pool_put(b, &m);
   if (rc != DSS_OK) return bfail(b, rc, "dss_batch_add: primitive-pair pool allocation failed");
+  rc = task_put(b, &m);
+  if (rc != DSS_OK) return bfail(b, rc, "dss_batch_add: task pool allocation failed");
   m.size = region_size(m.n, b->ds);
   size_t off = 0;
   if (!arena_alloc(b, m.size, &off))

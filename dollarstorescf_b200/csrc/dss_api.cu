@@ -530,7 +530,7 @@ void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector
     }
 }
 
-int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks) {
+int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks, bool no_tasks) {
   const int np = (int)P.pa.size();
   ctx->nbf = B.nbf;
   ctx->pure = B.pure;
@@ -571,6 +571,7 @@ int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks*
   ctx->class_pair0 = c0;
   ctx->class_pair1 = c1;
   ctx->basis = std::move(B);
+  if (no_tasks) return DSS_OK;
   if (tasks) return dss_install_tasks(ctx, *tasks);
   return dss_build_tasks(ctx);
 }
@@ -667,7 +668,11 @@ void dss_make_tasks(const std::vector<int>& c0, const std::vector<int>& c1, cons
   }
 }
 
-int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
+// Work lists of every class: counts, statistics, kernel shape and slices; with
+// host lists (ht) they are uploaded, else (counts, sq, pq) only size the device
+// buffers, which the caller fills on the context's stream.
+static int install_tasks(dss_ctx* ctx, const HostTasks* ht, const std::vector<int>* counts,
+                         const std::vector<long long>* sq, const std::vector<long long>* pq) {
   // The previous work-list buffers are reused (grow-only) by the new lists.
   std::vector<ClassTasks> old = std::move(ctx->tasks);
   ctx->tasks.clear();
@@ -687,7 +692,7 @@ int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
       ct.variant = ctx->class_variant[idx];
     else
       ct.variant = 0;  // thread per quartet; the tuner may pick other shapes
-    ct.ntasks = (int)ht.tasks[idx].size();
+    ct.ntasks = ht ? (int)ht->tasks[idx].size() : (*counts)[idx];
     // A single molecule whose class has few warp tasks (a small molecule) would
     // leave most SMs idle while each lane walks its quartet's whole primitive
     // product, so the thread-per-quartet launch is split into slices of the bra
@@ -698,10 +703,10 @@ int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
     // large molecules keep one slice.
     constexpr long long kSplitWarps = 4736;  // 148 SMs x 32 warps
     constexpr long long kSplitMinProduct = 64;
-    if (ctx->nmol == 0 && ct.ntasks > 0 && ct.ntasks < kSplitWarps) {
+    if (ht && ctx->nmol == 0 && ct.ntasks > 0 && ct.ntasks < kSplitWarps) {
       int max_npp = 1;
       long long longest = 1;
-      for (const int4& t : ht.tasks[idx])
+      for (const int4& t : ht->tasks[idx])
         if ((size_t)t.x < ctx->h_pair_npp.size() && (size_t)t.y < ctx->h_pair_npp.size()) {
           max_npp = std::max(max_npp, ctx->h_pair_npp[t.x]);
           longest = std::max(longest, (long long)ctx->h_pair_npp[t.x] * ctx->h_pair_npp[t.y]);
@@ -709,17 +714,30 @@ int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) {
       const long long want = (kSplitWarps + ct.ntasks - 1) / ct.ntasks;
       if (longest >= kSplitMinProduct) ct.split = (int)std::min<long long>(std::min<long long>(want, 32), max_npp);
     }
-    ct.shell_quartets = ht.shell_quartets[idx];
-    ct.prim_quartets = ht.prim_quartets[idx];
+    ct.shell_quartets = ht ? ht->shell_quartets[idx] : (*sq)[idx];
+    ct.prim_quartets = ht ? ht->prim_quartets[idx] : (*pq)[idx];
     ctx->n_warp_tasks += ct.ntasks;
     ctx->n_shell_quartets += ct.shell_quartets;
     ctx->n_prim_quartets += ct.prim_quartets;
     ctx->tasks.push_back(std::move(ct));
-    int rc_ = upload(ctx, ctx->tasks.back().d_tasks, ht.tasks[idx]);
-    if (rc_ != DSS_OK) return rc_;
+    if (ht) {
+      int rc_ = upload(ctx, ctx->tasks.back().d_tasks, ht->tasks[idx]);
+      if (rc_ != DSS_OK) return rc_;
+    } else {
+      DSS_CUDA(ctx->tasks.back().d_tasks.resize((size_t)std::max(ctx->tasks.back().ntasks, 1)));
+    }
   }
-  DSS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ht) DSS_CUDA(cudaStreamSynchronize(ctx->stream));
   return DSS_OK;
+}
+
+int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht) { return install_tasks(ctx, &ht, nullptr, nullptr, nullptr); }
+
+int dss_install_task_counts(dss_ctx* ctx, const std::vector<int>& counts, const std::vector<long long>& sq,
+                            const std::vector<long long>& pq) {
+  const size_t nq = sizeof(kQuartetClasses) / sizeof(kQuartetClasses[0]);
+  if (counts.size() != nq || sq.size() != nq || pq.size() != nq) return dss_fail(ctx, DSS_ERR_INVALID, "task counts");
+  return install_tasks(ctx, nullptr, &counts, &sq, &pq);
 }
 
 int dss_build_tasks(dss_ctx* ctx) {

@@ -220,7 +220,9 @@ void dss_pairs_merge(const std::vector<const PairSet*>& parts, const std::vector
 // context's basis (one molecule), in the order of its device primitive pairs.
 void dss_pair_alphas(const dss_ctx* ctx, std::vector<double>* alpha);
 // Makes B and P the context's basis: uploads, class ranges, work lists.
-int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks = nullptr);
+// no_tasks: install only the pairs (the caller installs the work lists).
+int dss_pairs_install(dss_ctx* ctx, BasisHost&& B, PairSet&& P, const HostTasks* tasks = nullptr,
+                      bool no_tasks = false);
 int dss_setup_pairs(dss_ctx* ctx, BasisHost&& B);
 // Shells from the C-ABI arrays: validation and the reference's primitive normalisation.
 int dss_make_basis(int n_shell, const int* l, const int* nprim, const double* exps, const double* coefs,
@@ -249,6 +251,10 @@ void dss_make_tasks(const std::vector<int>& c0, const std::vector<int>& c1, cons
                     const std::vector<int>& npp, const std::vector<int>& pmol, int nmol, double thr, HostTasks* out);
 // Uploads work lists as the context's (device buffers reused, grow-only).
 int dss_install_tasks(dss_ctx* ctx, const HostTasks& ht);
+// Work lists of the given per-class counts and statistics whose device buffers
+// (ctx->tasks[i].d_tasks, grow-only) the caller fills on the context's stream.
+int dss_install_task_counts(dss_ctx* ctx, const std::vector<int>& counts, const std::vector<long long>& sq,
+                            const std::vector<long long>& pq);
 // Number of shell-pair classes; bra and ket pair classes of quartet class i
 // (DSS_FOR_EACH_CLASS order).
 int dss_num_pair_classes();
