@@ -39,7 +39,7 @@ constexpr int kHdr = 256;
 enum Mat { M_H, M_S, M_X, M_D, M_DT, M_J, M_K, M_G, M_FN, M_F, M_T1, M_T2, M_CP, M_C, M_V, M_T3, M_GP, M_DP, M_NMAT };
 // Header slots
 constexpr int H_E = 0, H_EPREV = 1, H_TRDG = 2, H_ENUC = 3, H_DOTS = 4, H_COEF = 16, H_B = 32, H_TRDH = 140,
-              H_EFINAL = 141, H_INT = 200;
+              H_EFINAL = 141, H_XSCALE = 142, H_INT = 200;
 // Integer header (as int view of doubles from H_INT): iteration, done, diis count, diis slot, nocc, n, status,
 // final energy present; incremental form: iteration of the last full build, full builds in a row, final
 // phase reached, the current iteration is a full build.
@@ -525,6 +525,58 @@ __global__ void k_admit_init(double* base, int n, const double* Hp, const double
 }
 
 // out = V diag(eps)^-1/2 per molecule (eps: the molecule's eigenvalue slot).
+// X = S^-1/2 by the coupled Newton-Schulz iteration (Higham, Functions of
+// Matrices, 2008, eq. 6.35): Y0 = S/c, Z0 = I, T = (3 I - Z Y)/2, Y <- Y T,
+// Z <- T Z; Z -> (S/c)^-1/2 quadratically once Z Y is near I.  c = the largest
+// absolute row sum of S bounds its largest eigenvalue, so the iteration
+// converges.  One block per molecule sets c, Y0 and Z0.
+__global__ void k_ns_init(BatchView v, int ks, int ky, int kz) {
+  BV_BEGIN();
+  __shared__ double red[256];
+  const double* S = mat(base, n, ks);
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int j = 0; j < n; ++j) r += fabs(S[(size_t)i * n + j]);
+    m = fmax(m, r);
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  const double c = red[0];
+  for (long long t = threadIdx.x; t < n2; t += blockDim.x) {
+    mat(base, n, ky)[t] = S[t] / c;
+    mat(base, n, kz)[t] = (t / n == t % n) ? 1.0 : 0.0;
+  }
+  if (threadIdx.x == 0) base[H_XSCALE] = c;
+}
+
+// T = 1.5 I - 0.5 P, in place.
+__global__ void k_ns_t(BatchView v, int kp) {
+  BV_BEGIN();
+  double* P = mat(base, n, kp);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+    P[t] = (t / n == t % n ? 1.5 : 0.0) - 0.5 * P[t];
+}
+
+// X = Z / sqrt(c); *bad set when max |X S X - I| = max |P / c - I| exceeds tol
+// (P = Z S Z).
+__global__ void k_ns_finish(BatchView v, int kp, int kz, int kx, double tol, int* bad) {
+  BV_BEGIN();
+  const double* P = mat(base, n, kp);
+  const double c = base[H_XSCALE];
+  const double r = 1.0 / sqrt(c);
+  bool off = false;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+    mat(base, n, kx)[t] = mat(base, n, kz)[t] * r;
+    off = off || !(fabs(P[t] / c - (t / n == t % n ? 1.0 : 0.0)) <= tol);
+  }
+  if (off) atomicOr(bad, 1);
+}
+
 __global__ void k_scale_cols_eps(BatchView v, int kv, int kout) {
   BV_BEGIN();
   const double* w = eps_of(base, n, v.ds);
@@ -611,6 +663,7 @@ struct dss_batch {
   DevBuf<long long> d_region;
   DevBuf<int> d_n, d_active, d_active_next, d_nact;
   DevBuf<int> d_pending;  // per slot: 1 while the molecule's X is not computed
+  DevBuf<int> d_nsbad;    // set when the Newton-Schulz X of a new molecule did not converge
   DevBuf<double> admit_tmp;  // admission scratch (packed H, S, guess), grow-only
   PpPool pp_pool;
   TaskPool task_pool;
@@ -1006,9 +1059,37 @@ int prepare_x(dss_batch* b) {
   BatchView v = view(b, b->d_pending.ptr);
   const long long nn = (long long)b->nmax * b->nmax;
   const int tiles = (b->nmax + 31) / 32;
-  launch_jacobi(b, v, M_T1, M_V, M_T3, 60);  // M_T1 holds S since admission
-  k_scale_cols_eps<<<grid2(nn, nb), 256, 0, s>>>(v, M_V, M_T2);
-  k_gemm<<<dim3(tiles, tiles, nb), dim3(32, 8), 0, s>>>(v, M_T2, M_V, M_X, 0, 1, 1.0, 0.0);
+  const dim3 gg(tiles, tiles, nb), gb(32, 8);
+  // Newton-Schulz (batched GEMMs, no per-molecule serial sweeps): M_T1 holds S
+  // since admission; Y and Z alternate between (M_T2, M_T3) and (M_C, M_F),
+  // P = Z Y and T in M_V.  32 iterations converge for cond(S) c / lambda_max up
+  // to ~1e8; a molecule whose X S X is not I to 1e-11 afterwards sends the
+  // new molecules to the eigen-decomposition X = U s^-1/2 U^T below.
+  k_ns_init<<<dim3(1, nb), 256, 0, s>>>(v, M_T1, M_T2, M_T3);
+  int y = M_T2, z = M_T3, y2 = M_C, z2 = M_F;
+  for (int it = 0; it < 32; ++it) {
+    k_gemm<<<gg, gb, 0, s>>>(v, z, y, M_V, 0, 0, 1.0, 0.0);
+    k_ns_t<<<grid2(nn, nb), 256, 0, s>>>(v, M_V);
+    k_gemm<<<gg, gb, 0, s>>>(v, y, M_V, y2, 0, 0, 1.0, 0.0);
+    k_gemm<<<gg, gb, 0, s>>>(v, M_V, z, z2, 0, 0, 1.0, 0.0);
+    std::swap(y, y2);
+    std::swap(z, z2);
+  }
+  // The check is on X S X = Z S Z / c itself: S Z into the free buffer, then Z (S Z).
+  k_gemm<<<gg, gb, 0, s>>>(v, M_T1, z, y2, 0, 0, 1.0, 0.0);
+  k_gemm<<<gg, gb, 0, s>>>(v, z, y2, M_V, 0, 0, 1.0, 0.0);
+  if (b->d_nsbad.resize(1) != cudaSuccess) return DSS_ERR_OOM;
+  if (cudaMemsetAsync(b->d_nsbad.ptr, 0, sizeof(int), s) != cudaSuccess) return DSS_ERR_CUDA;
+  k_ns_finish<<<grid2(nn, nb), 256, 0, s>>>(v, M_V, z, M_X, 1e-11, b->d_nsbad.ptr);
+  int bad = 0;
+  if (cudaMemcpyAsync(&bad, b->d_nsbad.ptr, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return DSS_ERR_CUDA;
+  if (bad) {
+    launch_jacobi(b, v, M_T1, M_V, M_T3, 60);
+    k_scale_cols_eps<<<grid2(nn, nb), 256, 0, s>>>(v, M_V, M_T2);
+    k_gemm<<<gg, gb, 0, s>>>(v, M_T2, M_V, M_X, 0, 1, 1.0, 0.0);
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return DSS_ERR_CUDA;  // pend is freed on return
   for (int k = 0; k < nb; ++k) b->mols[b->slot_mol[k]].needs_x = false;
   return DSS_OK;
