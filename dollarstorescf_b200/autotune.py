@@ -149,6 +149,8 @@ def tune_whole(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, choice: Dict
             if names[i] in cache[key]["choice"]:
                 fb.set_class_variant(i, int(cache[key]["choice"][names[i]]))
                 choice[names[i]] = int(cache[key]["choice"][names[i]])
+        # The chosen shapes' launch times, which order the class launches of later builds.
+        fb.profile_build(D_ptr, J_ptr, K_ptr)
         return dict(cache[key]["result"], cached=True)
     per = fb.profile_build(D_ptr, J_ptr, K_ptr)
     order = sorted((i for i in range(nc) if infos[i][1] > 0 and names[i] in choice), key=lambda i: -per[i])
@@ -210,7 +212,10 @@ def tune_launch(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: in
 
 
 def tune_batch_launch(batch, repeats: int = 3) -> Dict[str, object]:
-    """tune_launch for a dss_batch (FP64 accumulation over all live molecules)."""
+    """tune_launch for a dss_batch (FP64 accumulation over all live molecules).
+    Profiles the current composition first: its class launch times order the
+    class launches of later builds."""
+    batch.profile()
     t = {}
     for on in (False, True):
         batch.set_persistent(on)

@@ -1539,7 +1539,10 @@ int dss_batch_profile(dss_batch* b, float* ms) {
   const cudaError_t e = cudaStreamSynchronize(s);
   if (rc == DSS_OK && e == cudaSuccess)
     for (int i = 0; i < nc && i < ncls; ++i)
-      if (ctx->tasks[i].ntasks) cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+      if (ctx->tasks[i].ntasks) {
+        cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+        dss_record_class_ms(ctx, i, ms[i]);
+      }
   for (auto& x : ev) cudaEventDestroy(x);
   ctx->d_mol_active = b->d_active.ptr;
   if (rc != DSS_OK) return bfail(b, rc, "dss_batch_profile: launch failed");

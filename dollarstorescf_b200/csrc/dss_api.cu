@@ -257,6 +257,7 @@ int dss_set_basis(dss_ctx* ctx, int n_shell, const int* l, const int* nprim, con
   ctx->nmol = 0;
   ctx->d_mol_active = nullptr;
   ctx->basis = B;
+  ctx->class_ms.clear();  // the launch times of another basis
   int rc = dss_setup_pairs(ctx, std::move(B));
   if (rc != DSS_OK) return rc;
   dss_preload_build(ctx);
@@ -762,9 +763,9 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
     DSS_CUDA(cudaMemsetAsync(Kacc, 0, nn * sizeof(double), ctx->stream));
     if (mode->uhf) DSS_CUDA(cudaMemsetAsync(mode->K2, 0, nn * sizeof(double), ctx->stream));
   }
-  // Launch order: highest total angular momentum first (longest per-quartet
-  // latency), spread round-robin over the side streams; profiling (events)
-  // keeps every launch on the main stream so each is timed alone.
+  // Launch order without measured times: highest total angular momentum first
+  // (longest per-quartet latency), spread round-robin over the side streams;
+  // profiling (events) keeps every launch on the main stream so each is timed alone.
   std::vector<int> order;
   for (size_t ci = 0; ci < ctx->tasks.size(); ++ci)
     if (ctx->tasks[ci].ntasks) order.push_back((int)ci);
@@ -853,9 +854,37 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
       DSS_CUDA(cudaGetLastError());
     }
   }
-  for (int ci : single) {
+  // Plain builds with a measured time alone for every class launch in its
+  // current shape (the last dss_profile_build, which times plain builds) order
+  // the launches longest first, each onto the side stream with the least work
+  // so far (longest-processing-time list scheduling), so that no stream ends
+  // with a long class started late.  The mixed and unrestricted forms run other
+  // kernels and keep the angular-momentum order (measured: the batched mixed
+  // form was slower under the plain form's times).
+  std::vector<int> lane(single.size(), -1);
+  if (fork && !mode->mixed && !mode->uhf && !ctx->class_ms.empty()) {
+    auto t = [&](int ci) {
+      const int vi = ctx->tasks[ci].variant;
+      return (size_t)ci < ctx->class_ms.size() && vi >= 0 && vi < 8 ? ctx->class_ms[ci][vi] : 0.0f;
+    };
+    bool have = true;
+    for (int ci : single) have = have && t(ci) > 0.0f;
+    if (have) {
+      std::stable_sort(single.begin(), single.end(), [&](int x, int y) { return t(x) > t(y); });
+      std::vector<float> load(ctx->nside, 0.0f);
+      for (size_t k = 0; k < single.size(); ++k) {
+        int best = 0;
+        for (int q = 1; q < ctx->nside; ++q)
+          if (load[q] < load[best]) best = q;
+        lane[k] = best;
+        load[best] += t(single[k]);
+      }
+    }
+  }
+  for (size_t si = 0; si < single.size(); ++si) {
+    const int ci = single[si];
     ClassTasks& ct = ctx->tasks[ci];
-    cudaStream_t st = fork ? ctx->side[slot++ % ctx->nside] : ctx->stream;
+    cudaStream_t st = fork ? ctx->side[lane[si] >= 0 ? lane[si] : (slot++ % ctx->nside)] : ctx->stream;
     EriArgs a{};
     common_args(a);
     a.tasks = ct.d_tasks.ptr;
@@ -1050,6 +1079,13 @@ int dss_time_build(dss_ctx* ctx, const double* D, double* J, double* K, float* m
   return rc;
 }
 
+extern "C++" void dss_record_class_ms(dss_ctx* ctx, int i, float ms) {
+  if (i < 0 || (size_t)i >= ctx->tasks.size()) return;
+  if (ctx->class_ms.size() < ctx->tasks.size()) ctx->class_ms.resize(ctx->tasks.size(), std::array<float, 8>{});
+  const int vi = ctx->tasks[i].variant;
+  if (vi >= 0 && vi < 8) ctx->class_ms[i][vi] = ms;
+}
+
 int dss_profile_build(dss_ctx* ctx, const double* D, double* J, double* K, float* ms) {
   if (!ctx || !ms) return DSS_ERR_INVALID;
   if (!ctx->nbf) return dss_fail(ctx, DSS_ERR_INVALID, "dss_profile_build: no basis set");
@@ -1073,7 +1109,10 @@ int dss_profile_build(dss_ctx* ctx, const double* D, double* J, double* K, float
   for (int i = 0; i < DSS_N_QUARTET_CLASSES; ++i) ms[i] = 0.0f;
   if (rc == DSS_OK)
     for (int i = 0; i < nc; ++i)
-      if (ctx->tasks[i].ntasks) cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+      if (ctx->tasks[i].ntasks) {
+        cudaEventElapsedTime(&ms[i], ev[2 * i], ev[2 * i + 1]);
+        dss_record_class_ms(ctx, i, ms[i]);
+      }
   for (auto& e : ev) cudaEventDestroy(e);
   return rc;
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <string>
 #include <vector>
 
@@ -117,6 +118,8 @@ struct dss_ctx {
   std::vector<double> h_Q;
   std::vector<int> class_pair0, class_pair1;
   std::vector<ClassTasks> tasks;
+  // Milliseconds of each class launch timed alone by the last profile, per kernel shape.
+  std::vector<std::array<float, 8>> class_ms;
   std::vector<int> class_variant;  // per class: -1 default, 0 thread, 1 warp-cooperative
   // Persistent grouped launches (dss_set_persistent) and their queue heads.
   bool persist = false;
@@ -290,5 +293,8 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
 // 1/4; UHF: D_alpha, D_beta, 1/2); shell_atom[s] the nucleus of shell s (host).
 int dss_eri_gradient_dense(dss_ctx* ctx, const double* D_dev, const double* X_dev, const double* Y_dev, double xfac,
                            int natom, const int* shell_atom, double* grad_host);
+// Keeps class i's launch time alone (ms) for its current kernel shape; the
+// class launches of later builds are ordered by these times (dss_enqueue_jk).
+void dss_record_class_ms(dss_ctx* ctx, int i, float ms);
 // Per shell-pair block maximum of |D| (dense n x n, device) into dmax [nshell^2].
 void dss_block_max(dss_ctx* ctx, const double* D, float* dmax);

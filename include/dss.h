@@ -157,7 +157,10 @@ int dss_kernels_per_build(const dss_ctx* ctx);
 
 /* One dss_build_jk_device with a CUDA event pair around every class launch;
  * ms_per_class[dss_num_classes()] receives each launch's device time (0 for
- * classes without work).  Synchronises the stream. */
+ * classes without work).  Synchronises the stream.  The context keeps the times
+ * per class and kernel shape (until the next dss_set_basis): once every class
+ * of a build has one for its current shape, plain builds launch the classes
+ * longest first, each onto the side stream with the least work so far. */
 int dss_profile_build(dss_ctx* ctx, const double* D_dense_dev, double* J_dense_dev, double* K_dense_dev,
                       float* ms_per_class);
 
