@@ -539,12 +539,12 @@ def run_gpu(args):
         "e2e": {"value": e2e_value, "unit": "builds/s", "h2d_bytes_per_step": npk * 8,
                 "d2h_bytes_per_step": 2 * npk * 8},
         "gpu_launches": kern * args.steps,
-        # The build's 21 class kernels run concurrently on six streams (the tuner's
+        # The build's 21 class kernels run concurrently on eight streams (the tuner's
         # shapes are chosen for that), so the roofline is the whole build's: its
         # algorithmic FLOP over its event-timed duration against the DFMA peak.
         # The dominant class launch, timed alone, is reported beside it.
         "roofline": {"bound": "fp64", "kernel": "Fock build: every class kernel (eri_jk_kernel / eri_coop_kernel), "
-                                                "concurrent on six streams",
+                                                "concurrent on eight side streams",
                      "achieved": build_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": build_tflops / peak if peak else None,
                      "peak_source": "measured in this run (dss_probe_fp64_peak DFMA loop)",

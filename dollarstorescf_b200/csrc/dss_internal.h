@@ -92,7 +92,7 @@ struct dss_ctx {
   // Side streams: the class launches of one build fork onto them so that the
   // long-running, low-occupancy high-angular-momentum classes overlap the rest.
   static constexpr int kSideStreams = 16;  // capacity; nside are used
-  int nside = 6;
+  int nside = 8;
   cudaStream_t side[kSideStreams] = {};
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[kSideStreams] = {};
