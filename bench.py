@@ -202,23 +202,28 @@ def measure_rows(device: int, cpu_baseline: bool):
 
 
 # ---------------------------------------------------------------- reference arm
-def _ref_worker(args):
-    seconds_budget, seed = args
+def _ref_init():
+    """Pool initializer: the reference's basis set-up, once per process."""
     sys.path.insert(0, ROOT)
     from oracle import refpy
 
     _, sh = _workload()
     refpy.setup(sh, build_tensor=False)
+
+
+def _ref_worker(args):
+    seconds_budget, seed = args
+    from oracle import refpy
+
     n, secs, _ = refpy.time_eri_random(seconds_budget, seed)
     return n, secs
 
 
-def reference_rate(budget_s: float = 12.0, cores: int = 0):
+def reference_rate(budget_s: float = 12.0, cores: int = 0, pool=None):
     """Reference ERI-phase throughput on the host cores, one process per core
-    (the reference's global state rules out threads).  Returns
-    (builds/s, quartets/s, cores, sample description)."""
-    import multiprocessing as mp
-
+    (the reference's global state rules out threads).  pool: a process pool
+    made by reference_pool (reused across samples), else one is made here.
+    Returns (builds/s, quartets/s, cores, sample description)."""
     from oracle import refpy
 
     if not refpy.available():
@@ -228,9 +233,16 @@ def reference_rate(budget_s: float = 12.0, cores: int = 0):
     npair = n * (n + 1) // 2
     total_quartets = npair * (npair + 1) // 2
     cores = cores or os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(budget_s, 1000003 * (k + 1)) for k in range(cores)])
+    own = pool is None
+    if own:
+        pool = reference_pool(cores)
+    try:
+        res = pool.map(_ref_worker, [(budget_s, 1000003 * (k + 1) + int(1e6 * time.perf_counter()) % 1000003)
+                                     for k in range(cores)])
+    finally:
+        if own:
+            pool.close()
+            pool.join()
     done = sum(r[0] for r in res)
     rate = sum(r[0] / r[1] for r in res if r[1] > 0)  # quartets/s over all processes
     builds = rate / total_quartets
@@ -238,6 +250,14 @@ def reference_rate(budget_s: float = 12.0, cores: int = 0):
               f"ERI phase (electronRepulsionIntegral), {cores} processes x {budget_s:.0f}s; scaled to one "
               f"full Fock build, ERI phase only")
     return builds, rate, cores, sample
+
+
+def reference_pool(cores: int = 0):
+    """One spawned process per host core, each with the reference's basis set up."""
+    import multiprocessing as mp
+
+    cores = cores or os.cpu_count() or 1
+    return mp.get_context("spawn").Pool(cores, initializer=_ref_init)
 
 
 def run_reference(args):
@@ -252,11 +272,18 @@ def run_reference(args):
     t_all = time.perf_counter()
     vals = []
     meta = None
-    for step in range(args.warmup + args.steps):
-        r = reference_rate(budget_s=6.0)
-        if step >= args.warmup:
-            vals.append(r[0])
-            meta = r
+    # One pool for every step (its processes set the basis up once); each step
+    # samples 2 s on every core, so the default 3 + 50 steps take about two minutes.
+    pool = reference_pool()
+    try:
+        for step in range(args.warmup + args.steps):
+            r = reference_rate(budget_s=2.0, pool=pool)
+            if step >= args.warmup:
+                vals.append(r[0])
+                meta = r
+    finally:
+        pool.close()
+        pool.join()
     v = statistics.mean(vals)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "builds/s", "n_gpus": ws,
