@@ -129,3 +129,28 @@ def test_persistent_launch_matches_reference(builders, name):
             assert np.abs(0.5 * K - d["K_rand"]).max() < 1e-10
     finally:
         fb.set_persistent(False)
+
+
+@pytest.mark.parametrize("name", ["dimer_631gs", "dimer_631gs_6d"])
+def test_list_scheduled_launches_match_reference(builders, name):
+    # After a profile the context knows every class's launch time, and plain
+    # builds launch the classes longest first onto the least-loaded side stream
+    # (two profiles: the times of more than one shape are kept).  J and K must
+    # not change.
+    import torch
+
+    d, mol, sh = load_case(name)
+    fb = builders[BOYS_REF]
+    n = fb.set_basis(sh)
+    D = torch.tensor(2.0 * shells.unpack(d["D_rand"], n), dtype=torch.float64, device="cuda:0")
+    J0, K0 = torch.empty_like(D), torch.empty_like(D)
+    fb.profile_build(D.data_ptr(), J0.data_ptr(), K0.data_ptr())
+    fb.set_class_variant(0, 2)
+    fb.profile_build(D.data_ptr(), J0.data_ptr(), K0.data_ptr())
+    try:
+        for _ in range(2):
+            J, K = fb.jk(2.0 * d["D_rand"])
+            assert np.abs(J - d["J_rand"]).max() < 1e-10
+            assert np.abs(0.5 * K - d["K_rand"]).max() < 1e-10
+    finally:
+        fb.set_class_variant(0, -1)

@@ -196,3 +196,25 @@ def test_whole_build_refinement_finds_the_concurrent_optimum():
     assert choice == {"a": 1, "b": 0, "c": 0}
     assert state == {0: 1, 1: 0, 2: 0}
     assert out["ms_whole_build_per_class_choice"] == 10.0 and out["ms_whole_build"] == 7.0
+
+
+@pytest.mark.parametrize("case", ["c4_631g", "c7_631g", "c10_631g", "c6_631gs", "w16_631gs", "w16_631gs_6d"])
+def test_newton_schulz_overlap_inverse_root_converges_in_32_iterations(case):
+    # The batch computes X = S^-1/2 of new molecules by 32 coupled Newton-Schulz
+    # iterations (Y0 = S/c, Z0 = I, T = (3I - ZY)/2, Y <- YT, Z <- TZ, X = Z/sqrt(c),
+    # c = the largest absolute row sum) and accepts X when max |X S X - I| <= 1e-11,
+    # else falls back to the eigen-decomposition.  The same arithmetic in numpy on
+    # the reference's own overlap matrices (alkanes of the batched form, the bench's
+    # water cluster) must pass that check and agree with U s^-1/2 U^T.
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", case + ".npz"))
+    n = int(d["nbf"])
+    S = d["S"] if d["S"].ndim == 2 else shells.unpack(d["S"], n)
+    c = np.abs(S).sum(axis=1).max()
+    Y, Z = S / c, np.eye(n)
+    for _ in range(32):
+        T = 1.5 * np.eye(n) - 0.5 * Z @ Y
+        Y, Z = Y @ T, T @ Z
+    X = Z / np.sqrt(c)
+    assert np.abs(X @ S @ X - np.eye(n)).max() <= 1e-11
+    w, U = np.linalg.eigh(S)
+    assert np.abs(X - (U / np.sqrt(w)) @ U.T).max() < 1e-9
