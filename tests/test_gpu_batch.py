@@ -54,6 +54,28 @@ def test_batch_continuous_join_and_leave():
     assert abs(done[h3] - float(d3["E"])) < 1e-9
 
 
+def test_batch_pools_compact_under_churn():
+    # Each admission appends the molecule's primitive pairs and work lists to
+    # the batch's device pools; removals leave holes, and a pool that fills up
+    # is compacted over the live molecules, moving their records.  Molecules
+    # admitted first stay live while 300 others join and leave (several
+    # compactions of both pools); their energies must still be the reference's.
+    cases = [load_case(n) for n in MIX]
+    _, _, churn = load_case("dimer_631gs")
+    with Batch(schwarz_threshold=0.0, boys_mode=BOYS_REF) as b:
+        hs = [b.add(sh) for (_, _, sh) in cases]
+        b.step(2, conv=1e-10)
+        for k in range(300):
+            h = b.add(churn)
+            if k % 50 == 0:
+                b.step(1, conv=1e-10)  # the composition is rebuilt over the moved records
+            b.remove(h)
+        b.solve(conv=1e-10)
+        out = [b.result(h)[0] for h in hs]
+    for (d, _, _), E in zip(cases, out):
+        assert abs(E - float(d["E"])) < 1e-9, (E, float(d["E"]))
+
+
 def test_batch_admission_by_memory():
     d, _, sh = load_case("dimer_631gs")
     with Batch(arena_bytes=600_000) as b:   # one 36-function molecule needs about 0.33 MB: one fits, two do not
