@@ -41,7 +41,7 @@ from typing import Dict, Optional
 from .engine import FockBuilder
 
 # Kernel shapes tried per class (see the module docstring).
-VARIANTS = (0, 2, 3, 1, 4, 5, 6, 7)
+VARIANTS = (0, 2, 3, 1, 4, 5, 6, 7, 8)
 
 
 def tune(fb: FockBuilder, D_ptr: int, J_ptr: int, K_ptr: int, repeats: int = 2,

@@ -65,6 +65,11 @@ def _class_tu(c, coop: bool) -> str:
     tiers = la + lb + lc + ld <= 4  # dss_has_tiers
     lines.append("  // tier 4..6: tiers 0..2 on a one-wave grid (the resident blocks of every SM; the")
     lines.append("  // warps stride over the tasks), which leaves room for the classes launched beside it.")
+    lines.append("  // tier 7: tier 0 on one block per SM of a third of the SMs, so that the local memory")
+    lines.append("  // of a class with large per-thread arrays stays within L2 (the rest of the SMs run")
+    lines.append("  // the classes beside it).")
+    lines.append("  const bool third = tier == 7;")
+    lines.append("  if (third) tier = 0;")
     lines.append("  const bool cap = tier >= 4;")
     lines.append("  if (cap) tier -= 4;")
     lines.append("  const int threads = 128;")
@@ -72,6 +77,8 @@ def _class_tu(c, coop: bool) -> str:
     lines.append("  if (!blocks) return;")
     lines.append(f"  if (cap) {{ const unsigned c = (unsigned)(dss_sm_count() * dss_min_blocks_tier({la + lb + lc + ld}, "
                  f"tier)); if (blocks > c) blocks = c; }}")
+    lines.append("  if (third) { const unsigned c = (unsigned)(dss_sm_count() / 3 > 0 ? dss_sm_count() / 3 : 1); "
+                 "if (blocks > c) blocks = c; }")
     lines.append("  const dim3 grid(blocks, a.split > 1 ? (unsigned)a.split : 1u);")
     for boys, pure, mixed in combos:
         pb = "true" if pure else "false"
@@ -276,7 +283,8 @@ def _dispatch_tu(classes, pcls, coop) -> str:
     for (la, lb, lc, ld) in classes:
         lines.append(f"void dss_preload_eri_jk_{la}{lb}{lc}{ld}(int boys, int pure, int variant);")
     lines.append("void dss_preload_eri_variant(int la, int lb, int lc, int ld, int boys, int pure, int variant) {")
-    lines.append("  if (variant >= 5) variant = variant == 5 ? 0 : variant - 3;  // one-wave grids: same kernels")
+    lines.append("  if (variant == 5 || variant == 8) variant = 0;  // capped grids: same kernels")
+    lines.append("  else if (variant >= 6) variant -= 3;")
     for (la, lb, lc, ld) in classes:
         lines.append(f"  if (la == {la} && lb == {lb} && lc == {lc} && ld == {ld}) "
                      f"return dss_preload_eri_jk_{la}{lb}{lc}{ld}(boys, pure, variant);")

@@ -865,7 +865,7 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   if (fork && !mode->mixed && !mode->uhf && !ctx->class_ms.empty()) {
     auto t = [&](int ci) {
       const int vi = ctx->tasks[ci].variant;
-      return (size_t)ci < ctx->class_ms.size() && vi >= 0 && vi < 8 ? ctx->class_ms[ci][vi] : 0.0f;
+      return (size_t)ci < ctx->class_ms.size() && vi >= 0 && vi < 9 ? ctx->class_ms[ci][vi] : 0.0f;
     };
     bool have = true;
     for (int ci : single) have = have && t(ci) > 0.0f;
@@ -995,7 +995,7 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* sq, long long*
 }
 
 int dss_set_class_variant(dss_ctx* ctx, int i, int variant) {
-  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 7) return DSS_ERR_INVALID;
+  if (!ctx || i < 0 || i >= DSS_N_QUARTET_CLASSES || variant < -1 || variant > 8) return DSS_ERR_INVALID;
   if (ctx->class_variant.size() < (size_t)DSS_N_QUARTET_CLASSES) ctx->class_variant.assign(DSS_N_QUARTET_CLASSES, -1);
   static const int kL[][4] = {
 #define DSS_CLASS_L2(a_, b_, c_, d_, e_, f_) {a_, b_, c_, d_},
@@ -1081,9 +1081,9 @@ int dss_time_build(dss_ctx* ctx, const double* D, double* J, double* K, float* m
 
 extern "C++" void dss_record_class_ms(dss_ctx* ctx, int i, float ms) {
   if (i < 0 || (size_t)i >= ctx->tasks.size()) return;
-  if (ctx->class_ms.size() < ctx->tasks.size()) ctx->class_ms.resize(ctx->tasks.size(), std::array<float, 8>{});
+  if (ctx->class_ms.size() < ctx->tasks.size()) ctx->class_ms.resize(ctx->tasks.size(), std::array<float, 9>{});
   const int vi = ctx->tasks[i].variant;
-  if (vi >= 0 && vi < 8) ctx->class_ms[i][vi] = ms;
+  if (vi >= 0 && vi < 9) ctx->class_ms[i][vi] = ms;
 }
 
 int dss_profile_build(dss_ctx* ctx, const double* D, double* J, double* K, float* ms) {

@@ -119,7 +119,7 @@ struct dss_ctx {
   std::vector<int> class_pair0, class_pair1;
   std::vector<ClassTasks> tasks;
   // Milliseconds of each class launch timed alone by the last profile, per kernel shape.
-  std::vector<std::array<float, 8>> class_ms;
+  std::vector<std::array<float, 9>> class_ms;
   std::vector<int> class_variant;  // per class: -1 default, 0 thread, 1 warp-cooperative
   // Persistent grouped launches (dss_set_persistent) and their queue heads.
   bool persist = false;

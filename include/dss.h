@@ -142,7 +142,10 @@ int dss_class_info(const dss_ctx* ctx, int i, int* l4, long long* shell_quartets
  * of total angular momentum <= 2; the plain FP64 reference-Boys build of an
  * unsplit launch, otherwise variant 0's kernel), 5, 6, 7 variants 0, 2, 3
  * launched as one wave (the blocks the SMs hold at once, the warps striding
- * over the work; 6 and 7 where 2 and 3 exist), -1 the library default
+ * over the work; 6 and 7 where 2 and 3 exist), 8 variant 0's kernel on one
+ * block per SM of a third of the SMs (a class whose per-thread arrays spill to
+ * local memory then keeps that memory within L2 while the other SMs run the
+ * classes beside it), -1 the library default
  * (variant 0: in a build the classes run concurrently, and the warp-cooperative
  * kernels' large shared-memory blocks slow the classes beside them more than
  * they gain, measured on the (H2O)16 6-31G* build 8.51 -> 7.21 ms).  Used

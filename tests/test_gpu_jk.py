@@ -100,7 +100,7 @@ def test_kernel_variants_agree(builders, name):
     fb.set_basis(sh)
     n = fb.num_classes()
     results = []
-    for variant in (0, 2, 3, 1, 4, 5, 6, 7):
+    for variant in (0, 2, 3, 1, 4, 5, 6, 7, 8):
         for i in range(n):
             try:
                 fb.set_class_variant(i, variant)
