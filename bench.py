@@ -534,6 +534,7 @@ def run_gpu(args):
     build_tflops = total_flops / (tot_ms / args.steps * 1e-3) / 1e12
     sq, pq, wt = fb.work_stats()
     traffic = None  # DRAM bytes per launch of the dominant kernel, from the committed ncu capture
+    build_traffic = None  # DRAM bytes of one whole build (sum of its launches' captures)
     tpath = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.isfile(tpath):
         with open(tpath) as f:
@@ -542,6 +543,8 @@ def run_gpu(args):
                 if len(p) == 2 and not ln.startswith("#") and \
                         p[0] == "eri_jk_kernel<%s>/%s" % (fl[dom]["class"], variants.get(fl[dom]["class"], 0)):
                     traffic = int(p[1])
+                if len(p) == 2 and not ln.startswith("#") and p[0] == "build":
+                    build_traffic = int(p[1])
     kern = fb.kernels_per_build()
     hbm_peak = None
     try:
@@ -575,8 +578,11 @@ def run_gpu(args):
                      "achieved": build_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": build_tflops / peak if peak else None,
                      "peak_source": "measured in this run (dss_probe_fp64_peak DFMA loop)",
-                     "traffic": None,
-                     "traffic_note": "DRAM bytes of the whole build are not captured; the dominant class's are below",
+                     "traffic": build_traffic,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum summed over the 21 class launches "
+                                       "of one build, each captured from a flushed L2 (an upper bound), from the "
+                                       "committed ncu capture of this workload (profiles/traffic.txt, "
+                                       "build_dram_h2o16_631gs.md), not measured in this run",
                      "dominant_kernel_alone": {
                          "kernel": "eri_jk_kernel<%s>" % fl[dom]["class"], "shape": variants.get(fl[dom]["class"]),
                          "achieved": achieved, "frac": achieved / peak if peak else None,
