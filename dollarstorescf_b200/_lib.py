@@ -80,6 +80,8 @@ def load():
     L.dss_get_stream.restype = vp
     L.dss_num_classes.argtypes = []
     L.dss_num_classes.restype = ctypes.c_int
+    L.dss_list_schedule.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int, ip, ip]
+    L.dss_list_schedule.restype = ctypes.c_int
     L.dss_class_info.argtypes = [vp, ctypes.c_int, ip, llp, llp, llp]
     L.dss_class_info.restype = ctypes.c_int
     L.dss_kernels_per_build.argtypes = [vp]

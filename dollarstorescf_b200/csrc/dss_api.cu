@@ -857,28 +857,25 @@ int dss_enqueue_jk(dss_ctx* ctx, const double* D, double* Jacc, double* Kacc, cu
   // Plain builds with a measured time alone for every class launch in its
   // current shape (the last dss_profile_build, which times plain builds) order
   // the launches longest first, each onto the side stream with the least work
-  // so far (longest-processing-time list scheduling), so that no stream ends
-  // with a long class started late.  The mixed and unrestricted forms run other
-  // kernels and keep the angular-momentum order (measured: the batched mixed
-  // form was slower under the plain form's times).
+  // so far (dss_list_schedule), so that no stream ends with a long class
+  // started late.  The mixed and unrestricted forms run other kernels (the
+  // incremental builds skip a different share of each class) and keep the
+  // angular-momentum order.
   std::vector<int> lane(single.size(), -1);
   if (fork && !mode->mixed && !mode->uhf && !ctx->class_ms.empty()) {
-    auto t = [&](int ci) {
-      const int vi = ctx->tasks[ci].variant;
-      return (size_t)ci < ctx->class_ms.size() && vi >= 0 && vi < 9 ? ctx->class_ms[ci][vi] : 0.0f;
-    };
+    std::vector<float> t(single.size());
     bool have = true;
-    for (int ci : single) have = have && t(ci) > 0.0f;
+    for (size_t k = 0; k < single.size(); ++k) {
+      const int ci = single[k], vi = ctx->tasks[ci].variant;
+      t[k] = (size_t)ci < ctx->class_ms.size() && vi >= 0 && vi < 9 ? ctx->class_ms[ci][vi] : 0.0f;
+      have = have && t[k] > 0.0f;
+    }
     if (have) {
-      std::stable_sort(single.begin(), single.end(), [&](int x, int y) { return t(x) > t(y); });
-      std::vector<float> load(ctx->nside, 0.0f);
-      for (size_t k = 0; k < single.size(); ++k) {
-        int best = 0;
-        for (int q = 1; q < ctx->nside; ++q)
-          if (load[q] < load[best]) best = q;
-        lane[k] = best;
-        load[best] += t(single[k]);
-      }
+      std::vector<int> order(single.size());
+      dss_list_schedule(t.data(), (int)t.size(), ctx->nside, order.data(), lane.data());
+      std::vector<int> sorted(single.size());
+      for (size_t k = 0; k < single.size(); ++k) sorted[k] = single[order[k]];
+      single = sorted;
     }
   }
   for (size_t si = 0; si < single.size(); ++si) {
@@ -975,6 +972,21 @@ int dss_set_stream(dss_ctx* ctx, void* stream) {
 }
 
 void* dss_get_stream(const dss_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int dss_list_schedule(const float* ms, int n, int nstreams, int* order, int* stream) {
+  if (n < 0 || nstreams < 1 || (n > 0 && (!ms || !order || !stream))) return DSS_ERR_INVALID;
+  for (int k = 0; k < n; ++k) order[k] = k;
+  std::stable_sort(order, order + n, [&](int x, int y) { return ms[x] > ms[y]; });
+  std::vector<double> load(nstreams, 0.0);
+  for (int k = 0; k < n; ++k) {
+    int best = 0;
+    for (int q = 1; q < nstreams; ++q)
+      if (load[q] < load[best]) best = q;
+    stream[k] = best;
+    load[best] += ms[order[k]];
+  }
+  return DSS_OK;
+}
 
 int dss_num_classes(void) { return DSS_N_QUARTET_CLASSES; }
 

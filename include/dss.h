@@ -155,6 +155,12 @@ int dss_set_class_variant(dss_ctx* ctx, int i, int variant);
 /* The variant class i currently runs with (-1 before a basis is set). */
 int dss_get_class_variant(const dss_ctx* ctx, int i);
 
+/* The list schedule of a plain build's class launches (host only): n launch
+ * times ms[] and nstreams side streams; order[k] is the index of the k-th
+ * launch (longest first, ties in index order) and stream[k] its side stream,
+ * the one with the least work so far (lowest index on ties). */
+int dss_list_schedule(const float* ms, int n, int nstreams, int* order, int* stream);
+
 /* Kernel launches one dss_build_jk_device call enqueues. */
 int dss_kernels_per_build(const dss_ctx* ctx);
 
